@@ -1,0 +1,224 @@
+/*
+ * num_b200.h -- C ABI of the num_b200 sparse library (CSR SpMV, multi-RHS and
+ * many-matrix SpMV, CG and its vector ops, halo pack/unpack), built for
+ * NVIDIA B200 (sm_100a).
+ *
+ * This is the drop-in boundary for the `kokkos_spmv` Python module of
+ * w-jiwonchoi/num (src/bindings.cpp).  Every entry point takes plain pointers
+ * and sizes; device buffers are raw CUDA device pointers and `stream` is a
+ * cudaStream_t (NULL = the legacy default stream).  Entry points that only
+ * enqueue work return as soon as it is enqueued; the ones that return a host
+ * scalar (nm_dot, nm_norm2, nm_cg_*) synchronise `stream` first.
+ *
+ * Every function returns an nm_status; on failure nm_last_error() returns a
+ * message for the calling thread.  The Python binding maps NM_ERR_INVALID to
+ * ValueError, NM_ERR_TYPE to TypeError and the rest to RuntimeError, which are
+ * the exception types of the reference binding.
+ */
+#ifndef NUM_B200_H
+#define NUM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status, dtypes, result records ------------------------------------ */
+
+enum nm_status {
+    NM_OK = 0,
+    NM_ERR_INVALID = 1,   /* bad size / shape / index: std::invalid_argument   */
+    NM_ERR_TYPE = 2,      /* unsupported dtype                                  */
+    NM_ERR_RUNTIME = 3,   /* algorithmic failure (e.g. CG breakdown guard)      */
+    NM_ERR_CUDA = 4,      /* CUDA runtime error                                 */
+    NM_ERR_NOMEM = 5      /* device allocation failed                           */
+};
+
+enum nm_dtype { NM_F64 = 0, NM_F32 = 1, NM_BF16 = 2 };
+
+/* CGResult (src/cg_solver.hpp:22-26). */
+typedef struct {
+    int32_t iters;
+    double final_res;
+    int32_t converged;
+} nm_cg_result;
+
+/* Row-block partition parameters of the SpMV kernels (see nm_csr_set_tuning). */
+typedef struct {
+    int32_t tile;       /* max nonzeros of a multi-row block; longer rows get a CTA */
+    int32_t max_rows;   /* max rows of a block (<= 256)                             */
+    int32_t short_max;  /* rows with <= short_max nonzeros: one thread; else a warp */
+    int32_t grid_mult;  /* CTAs launched per SM by the persistent SpMV grid (0: auto) */
+} nm_tuning;
+
+typedef struct nm_csr nm_csr;    /* device CSR matrix (CrsMatrixHandle)   */
+typedef struct nm_dist nm_dist;  /* one rank's slice (DistCrsHandle)      */
+
+/* ---- errors / context ----------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* nm_last_error(void);
+
+/* Library version string. */
+const char* nm_version(void);
+
+/* init(device_id) (src/bindings.cpp:53-66): selects the device and creates
+ * its context.  This library is one process per GPU; rank/size are 0/1 here
+ * (the Python layer reports torch.distributed's values when it is set up). */
+int nm_init(int device_id, int32_t* rank, int32_t* size);
+
+/* finalize() (src/bindings.cpp:68-70): releases cached workspaces. */
+int nm_finalize(void);
+
+/* ---- CSR matrix ------------------------------------------------------------ */
+
+/* CrsMatrixHandle ctor (src/crs_matrix.hpp:45-72) / upload_csr
+ * (src/bindings.cpp:97-108).  Copies host CSR arrays (int32 row_ptr[n+1],
+ * int32 col_idx[nnz], values[nnz] of `dtype`) to the device and builds the
+ * row-block partition.  nnz = row_ptr[nrows].  Non-positive dims, a row_ptr
+ * that does not start at 0 or decreases, and column indices outside
+ * [0, ncols) return NM_ERR_INVALID. */
+int nm_csr_create(const int32_t* row_ptr, const int32_t* col_idx, const void* values,
+                  int dtype, int32_t nrows, int32_t ncols, nm_csr** out);
+
+/* Many independent CSR matrices (no counterpart in the reference): matrix m
+ * has dims (nrows[m], ncols[m]) and its own CSR arrays, concatenated in
+ * matrix order: row_ptr holds count segments of nrows[m]+1 entries (each
+ * starting at 0), col_idx/values hold the nonzeros with LOCAL column indices.
+ * The result is one block-diagonal device matrix; x and y of nm_spmv are the
+ * per-matrix vectors concatenated in matrix order, so one launch multiplies
+ * every matrix. */
+int nm_csr_create_batched(int32_t count, const int32_t* nrows, const int32_t* ncols,
+                          const int32_t* row_ptr, const int32_t* col_idx,
+                          const void* values, int dtype, nm_csr** out);
+
+/* Frees the device copy (handle destructor). */
+int nm_csr_destroy(nm_csr* A);
+
+/* Read-only properties nrows/ncols/nnz (src/bindings.cpp:79-88), the value
+ * dtype, and the number of row blocks. */
+int nm_csr_info(const nm_csr* A, int32_t* nrows, int32_t* ncols, int32_t* nnz,
+                int32_t* dtype, int32_t* nblocks);
+
+/* Replaces pick_rows_per_team (src/spmv_kernel.hpp:102-109): sets the
+ * row-block partition parameters and rebuilds the partition.  Fields <= 0
+ * keep their defaults (2048, 256, 32, auto). */
+int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t);
+int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t);
+
+/* Copies the row-block boundaries (nblocks+1 entries) and, if bins != NULL,
+ * the per-row reduction bin (0 thread, 1 warp, 2 CTA) to host memory. */
+int nm_csr_row_blocks(const nm_csr* A, int32_t* blk, int32_t cap, int8_t* bins);
+
+/* Host only (needs no GPU): the row-block partition nm_csr_create builds for
+ * row_ptr under tuning t (NULL = defaults); *nblk receives the block count,
+ * blk its nblk+1 boundaries, bins (optional) the per-row reduction bin. */
+int nm_row_blocks_host(const int32_t* row_ptr, int32_t nrows, const nm_tuning* t,
+                       int32_t* blk, int32_t cap, int8_t* bins, int32_t* nblk);
+
+/* ---- SpMV ------------------------------------------------------------------ */
+
+/* spmv(A, x, y) (src/bindings.cpp:152-170; launch_spmv_custom and
+ * launch_spmv_kokkoskernels, src/spmv_kernel.hpp:118-180): y = A*x.
+ * F64 matrices take double x/y; F32 and BF16 matrices take float x/y and
+ * accumulate in FP32. */
+int nm_spmv(const nm_csr* A, const void* x, void* y, void* stream);
+
+/* batch_spmv(A, X, Y) (src/bindings.cpp:186-200; launch_batch_spmv,
+ * src/batch_spmv_kernel.hpp:120-174): Y(nrows,k) = A * X(ncols,k), both
+ * row-major.  F64 matrices only (as in the reference). */
+int nm_batch_spmv(const nm_csr* A, const double* X, double* Y, int32_t k, void* stream);
+
+/* ---- vector ops (src/vec_ops.hpp) ------------------------------------------- */
+
+/* vec_axpy (src/vec_ops.hpp:16-26): z = alpha*x + y, one FMA. */
+int nm_axpy(int64_t n, double alpha, const double* x, const double* y, double* z,
+            void* stream);
+/* vec_axpy2 (src/vec_ops.hpp:31-42): z = alpha*x + beta*y = fma(beta, y, alpha*x). */
+int nm_axpy2(int64_t n, double alpha, const double* x, double beta, const double* y,
+             double* z, void* stream);
+/* vec_local_dot (src/vec_ops.hpp:47-59): deterministic sum of x[i]*y[i]. */
+int nm_dot(int64_t n, const double* x, const double* y, double* result, void* stream);
+/* vec_local_norm2 (src/vec_ops.hpp:64-69). */
+int nm_norm2(int64_t n, const double* x, double* result, void* stream);
+/* vec_copy / vec_fill / vec_scale (src/vec_ops.hpp:74-100). */
+int nm_copy(int64_t n, const double* src, double* dst, void* stream);
+int nm_fill(int64_t n, double value, double* x, void* stream);
+int nm_scale(int64_t n, double alpha, double* x, void* stream);
+
+/* ---- CG -------------------------------------------------------------------- */
+
+/* cg_solve_local (src/cg_solver.hpp:133-196; src/bindings.cpp:273-290):
+ * unpreconditioned CG, x in/out, same stopping rule and iteration count.
+ * The iteration runs on the device with device-resident scalars; the
+ * workspace is cached on the matrix.  F64 matrices. */
+int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter,
+                nm_cg_result* result, void* stream);
+
+/* ---- distributed slice, halo pack / unpack -------------------------------- */
+
+/* distribute_csr (src/dist_spmv.hpp:27-100; build_ghost_map
+ * src/halo_exchange.hpp:38-130; build_send_indices :154-191) for rank `rank`
+ * of `size`: even block-row split, local CSR with columns remapped to
+ * [0, local_n + n_ghost), ghost lists per owner rank (ascending ids, offsets
+ * in owner-rank order) and send index lists.  Host work plus one upload. */
+int nm_dist_create(const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                   int32_t global_nrows, int32_t global_ncols, int32_t rank, int32_t size,
+                   nm_dist** out);
+int nm_dist_destroy(nm_dist* D);
+
+/* Host only (needs no GPU): the same partition and halo plan as
+ * nm_dist_create without any device upload.  Such a handle answers the
+ * info / plan / local_host queries; compute entry points reject it. */
+int nm_dist_plan(const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                 int32_t global_nrows, int32_t global_ncols, int32_t rank, int32_t size,
+                 nm_dist** out);
+
+/* Host copy of the remapped local CSR (row_ptr local_n+1, col_idx/values
+ * local_nnz); pass NULL arrays to query *local_nnz first. */
+int nm_dist_local_host(const nm_dist* D, int32_t* local_nnz, int32_t* row_ptr,
+                       int32_t* col_idx, double* values);
+
+/* DistCrsMatrix properties (src/bindings.cpp:90-94) plus the halo sizes. */
+int nm_dist_info(const nm_dist* D, int32_t* global_nrows, int32_t* row_start,
+                 int32_t* row_end, int32_t* n_ghost, int32_t* total_send,
+                 int32_t* n_send_nbrs, int32_t* n_recv_nbrs);
+
+/* Host copies of the exchange plan: per neighbour its rank, count and offset
+ * (send: offset into the packed send buffer; recv: offset of its ghosts in
+ * x_ghost), and the flat lists (send: LOCAL indices packed in neighbour
+ * order; recv: GLOBAL ghost ids in ghost order).  Arrays sized from
+ * nm_dist_info. */
+int nm_dist_send_plan(const nm_dist* D, int32_t* nbr_rank, int32_t* count, int32_t* offset,
+                      int32_t* send_idx);
+int nm_dist_recv_plan(const nm_dist* D, int32_t* nbr_rank, int32_t* count, int32_t* offset,
+                      int32_t* ghost_ids);
+
+/* The local matrix (columns in [0, local_n + n_ghost)); owned by D. */
+int nm_dist_local(const nm_dist* D, const nm_csr** local);
+
+/* halo_pack (src/halo_exchange.hpp:228-233): send_buf[i] = x_local[send_idx[i]]. */
+int nm_halo_pack(const nm_dist* D, const double* x_local, double* send_buf, void* stream);
+
+/* halo_scatter (src/halo_exchange.hpp:289-298) for all neighbours at once:
+ * x_ext[local_n + off_r + i] = recv_buf[off_r + i], with recv_buf holding the
+ * neighbours' values back to back in ghost order. */
+int nm_halo_unpack(const nm_dist* D, const double* recv_buf, double* x_ext, void* stream);
+
+/* distributed_spmv local part (src/dist_spmv.hpp:118-163): y_local = A_local *
+ * x_ext, x_ext = [x_local | x_ghost].  With no ghosts x_ext may be x_local. */
+int nm_dist_spmv_local(const nm_dist* D, const double* x_ext, double* y_local, void* stream);
+
+/* cg_solve_distributed (src/cg_solver.hpp:38-125) at one rank (no ghosts):
+ * CG of nm_cg_local plus the reference's breakdown guard |p.Ap| < 1e-300,
+ * reported as NM_ERR_RUNTIME "CG: p'Ap is near zero - A may not be SPD". */
+int nm_dist_cg_single(nm_dist* D, const double* b, double* x, double tol, int32_t max_iter,
+                      nm_cg_result* result, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUM_B200_H */

@@ -1,0 +1,91 @@
+// api.cu -- error reporting, device context, host-only helpers.
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "csr.cuh"
+
+namespace nm {
+
+namespace {
+thread_local std::string g_last_error;
+std::mutex g_sm_mu;
+std::unordered_map<int, int> g_sm_count;
+}  // namespace
+
+int fail(int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return status;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+int sm_count() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+    std::lock_guard<std::mutex> g(g_sm_mu);
+    auto it = g_sm_count.find(dev);
+    if (it != g_sm_count.end()) return it->second;
+    int n = 1;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+        n = 1;
+    g_sm_count[dev] = n;
+    return n;
+}
+
+void release_dot_scratch();  // vec.cu
+
+}  // namespace nm
+
+using nm::fail;
+
+extern "C" const char* nm_last_error(void) { return nm::g_last_error.c_str(); }
+
+extern "C" const char* nm_version(void) { return "num_b200 0.1.0 (sm_100a)"; }
+
+extern "C" int nm_init(int device_id, int32_t* rank, int32_t* size) {
+    nm::clear_error();
+    int n = 0;
+    NM_CUDA_TRY(cudaGetDeviceCount(&n));
+    if (device_id < 0 || device_id >= n)
+        return fail(NM_ERR_INVALID, "init: device_id %d outside [0, %d)", device_id, n);
+    NM_CUDA_TRY(cudaSetDevice(device_id));
+    NM_CUDA_TRY(cudaFree(nullptr));  // create the context now
+    if (rank) *rank = 0;
+    if (size) *size = 1;
+    return NM_OK;
+}
+
+extern "C" int nm_finalize(void) {
+    nm::clear_error();
+    nm::release_dot_scratch();
+    return NM_OK;
+}
+
+// Host-only: the row-block partition nm_csr_create would build for `row_ptr`
+// under tuning `t` (NULL = defaults).  Needs no GPU.
+extern "C" int nm_row_blocks_host(const int32_t* row_ptr, int32_t nrows, const nm_tuning* t,
+                                  int32_t* blk, int32_t cap, int8_t* bins, int32_t* nblk) {
+    nm::clear_error();
+    if (!row_ptr || !blk || !nblk || nrows < 0)
+        return fail(NM_ERR_INVALID, "nm_row_blocks_host: bad argument");
+    nm_tuning tt = t ? *t : nm_tuning{0, 0, 0, 0};
+    if (tt.tile <= 0) tt.tile = nm::kDefaultTile;
+    if (tt.max_rows <= 0) tt.max_rows = nm::kDefaultMaxRows;
+    if (tt.short_max <= 0) tt.short_max = nm::kDefaultShortMax;
+    std::vector<int32_t> b;
+    std::vector<int8_t> bn;
+    const int nb = nm::build_row_blocks(row_ptr, nrows, tt.tile, tt.max_rows, tt.short_max, b,
+                                        bins ? &bn : nullptr);
+    if (nb + 1 > cap) return fail(NM_ERR_INVALID, "nm_row_blocks_host: cap %d < %d", cap, nb + 1);
+    std::copy(b.begin(), b.end(), blk);
+    if (bins && !bn.empty()) std::copy(bn.begin(), bn.end(), bins);
+    *nblk = nb;
+    return NM_OK;
+}

@@ -1,0 +1,283 @@
+// cg.cu -- conjugate gradient with device-resident scalars.
+//
+// Same algorithm, stopping rule and iteration count as cg_solve_local
+// (src/cg_solver.hpp:133-196) and, with the breakdown guard, as
+// cg_solve_distributed at one rank (src/cg_solver.hpp:38-125).  The reference
+// runs 5 launches, 5 fences and 2 device->host scalar copies per iteration;
+// here one iteration is three kernels that never return to the host:
+//
+//   K1 spmv_pap : Ap = A p fused with p.Ap (row epilogue); last CTA: alpha
+//   K2 update_xr: x += alpha p, r -= alpha Ap, r.r; last CTA: stopping test,
+//                 beta, iteration count
+//   K3 update_p : p = r + beta p
+//
+// Each kernel returns at once when the solve is done, so the host enqueues
+// iterations in CUDA-graph chunks and polls the done flag between chunks.
+// HBM per iteration: 12 nnz + 4(n+1) (matrix) + 8n (p gather, L2-resident
+// in steady state) + 8n (Ap write) in K1; 4 reads + 2 writes of n doubles in
+// K2; 2 reads + 1 write in K3 -- 12 nnz + 4(n+1) + 88 n bytes.
+#include <cmath>
+#include <cstring>
+
+#include "cg.cuh"
+#include "spmv.cuh"
+
+namespace nm {
+
+__global__ void __launch_bounds__(kThreads)
+    cg_init_kernel(int64_t n, CgState* st, const double* __restrict__ Ap, double* __restrict__ r,
+                   double* __restrict__ p, double* partials) {
+    __shared__ double red[kWarps];
+    const double* __restrict__ b = st->b;
+    double srr = 0.0, sbb = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * kThreads + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kThreads) {
+        const double bi = b[i];
+        const double ri = fma(-1.0, Ap[i], bi);  // r = -1*Ap + b
+        r[i] = ri;
+        p[i] = ri;
+        srr = fma(ri, ri, srr);
+        sbb = fma(bi, bi, sbb);
+    }
+    double part[2];
+    part[0] = block_sum(srr, red);
+    part[1] = block_sum(sbb, red);
+    double tot[2];
+    if (grid_reduce_last<2>(part, partials, &st->counter, tot, red)) {
+        const double rr = tot[0];
+        double bnorm = sqrt(tot[1]);
+        if (bnorm == 0.0) bnorm = 1.0;
+        st->bnorm = bnorm;
+        st->rr = rr;
+        st->iter = 0;
+        st->status = kCgOk;
+        const double rel = sqrt(rr) / bnorm;
+        if (rel < st->tol) {
+            st->done = 1; st->converged = 1; st->iters = 0; st->final_res = rel;
+        } else if (st->max_iter <= 0) {
+            st->done = 1; st->converged = 0; st->iters = st->max_iter; st->final_res = rel;
+        } else {
+            st->done = 0; st->converged = 0;
+        }
+    }
+}
+
+// Row epilogue of K1: store Ap and accumulate p.Ap.
+struct PApEpi {
+    double* __restrict__ Ap;
+    const double* __restrict__ p;
+    double dot;
+    __device__ __forceinline__ void operator()(int32_t row, double v) {
+        Ap[row] = v;
+        dot = fma(__ldg(p + row), v, dot);
+    }
+};
+
+template <int TILE>
+__global__ void __launch_bounds__(kThreads)
+    cg_spmv_pap_kernel(const CsrView<double> M, CgState* st, const double* __restrict__ p,
+                       double* __restrict__ Ap, double* partials) {
+    if (__ldcg(&st->done)) return;
+    __shared__ SpmvSmem<double, TILE> sm;
+    PApEpi epi{Ap, p, 0.0};
+    for (int32_t b = blockIdx.x; b < M.nblk; b += gridDim.x)
+        spmv_block<double, double, double, TILE>(M, M.blk[b], M.blk[b + 1], p, sm, epi);
+    double part[1] = {block_sum(epi.dot, sm.red)};
+    double tot[1];
+    if (grid_reduce_last<1>(part, partials, &st->counter, tot, sm.red)) {
+        const double pAp = tot[0];
+        st->pAp = pAp;
+        if (st->guard && fabs(pAp) < 1e-300) {
+            st->status = kCgBreakdown;
+            st->done = 1;
+            st->converged = 0;
+            st->iters = st->iter;
+            st->final_res = sqrt(st->rr) / st->bnorm;
+        } else {
+            st->alpha = st->rr / pAp;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    cg_update_xr_kernel(int64_t n, CgState* st, const double* __restrict__ p,
+                        const double* __restrict__ Ap, double* __restrict__ r, double* partials) {
+    if (__ldcg(&st->done)) return;
+    __shared__ double red[kWarps];
+    const double alpha = __ldcg(&st->alpha);
+    double* __restrict__ x = st->x;
+    double s = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * kThreads + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kThreads) {
+        const double pi = p[i];
+        x[i] = fma(alpha, pi, x[i]);            // x = alpha*p + x
+        const double ri = fma(-alpha, Ap[i], r[i]);  // r = -alpha*Ap + r
+        r[i] = ri;
+        s = fma(ri, ri, s);
+    }
+    double part[1] = {block_sum(s, red)};
+    double tot[1];
+    if (grid_reduce_last<1>(part, partials, &st->counter, tot, red)) {
+        const double rr_new = tot[0];
+        const int32_t it = st->iter + 1;
+        st->iter = it;
+        const double rel = sqrt(rr_new) / st->bnorm;
+        if (rel < st->tol) {
+            st->done = 1; st->converged = 1; st->iters = it; st->final_res = rel;
+        } else {
+            if (it >= st->max_iter) {
+                st->done = 1; st->converged = 0; st->iters = st->max_iter; st->final_res = rel;
+            }
+            st->beta = rr_new / st->rr;
+            st->rr = rr_new;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    cg_update_p_kernel(int64_t n, const CgState* st, double* __restrict__ p,
+                       const double* __restrict__ r) {
+    if (__ldcg(&st->done)) return;
+    const double beta = __ldcg(&st->beta);
+    for (int64_t i = int64_t(blockIdx.x) * kThreads + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kThreads)
+        p[i] = fma(beta, p[i], r[i]);  // p = 1*r + beta*p
+}
+
+CgWorkspace::~CgWorkspace() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    cudaFree(r);
+    cudaFree(p);
+    cudaFree(Ap);
+    cudaFree(partials);
+    cudaFree(st);
+    cudaFreeHost(h_in);
+    cudaFreeHost(h_out);
+}
+
+namespace {
+
+int ensure_workspace(nm_csr* A, CgWorkspace** out) {
+    if (A->cg) {
+        *out = A->cg.get();
+        return NM_OK;
+    }
+    auto ws = std::make_unique<CgWorkspace>();
+    const int64_t n = A->nrows;
+    ws->n = n;
+    ws->grid_spmv = spmv_grid(A, 8);
+    ws->grid_vec = vec_grid(n);
+    ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
+    NM_CUDA_TRY(cudaMalloc(&ws->r, sizeof(double) * size_t(n)));
+    NM_CUDA_TRY(cudaMalloc(&ws->p, sizeof(double) * size_t(n)));
+    NM_CUDA_TRY(cudaMalloc(&ws->Ap, sizeof(double) * size_t(n)));
+    NM_CUDA_TRY(cudaMalloc(&ws->partials, sizeof(double) * size_t(ws->partials_cap)));
+    NM_CUDA_TRY(cudaMalloc(&ws->st, sizeof(CgState)));
+    NM_CUDA_TRY(cudaMemset(ws->st, 0, sizeof(CgState)));
+    NM_CUDA_TRY(cudaMallocHost(&ws->h_in, sizeof(CgState)));
+    NM_CUDA_TRY(cudaMallocHost(&ws->h_out, sizeof(CgState)));
+    NM_CUDA_TRY(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
+    A->cg = std::move(ws);
+    *out = A->cg.get();
+    return NM_OK;
+}
+
+template <int TILE>
+void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    const CsrView<double> M = A->view<double>();
+    cg_spmv_pap_kernel<TILE><<<ws->grid_spmv, kThreads, 0, s>>>(M, ws->st, ws->p, ws->Ap,
+                                                                 ws->partials);
+    cg_update_xr_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->p, ws->Ap, ws->r,
+                                                          ws->partials);
+    cg_update_p_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->p, ws->r);
+}
+
+void launch_iteration(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    switch (A->tune.tile) {
+        case 1024: launch_iteration_t<1024>(A, ws, s); break;
+        case 4096: launch_iteration_t<4096>(A, ws, s); break;
+        default: launch_iteration_t<2048>(A, ws, s); break;
+    }
+}
+
+// A CUDA graph of `iters` CG iterations (3 kernels each), captured once per
+// workspace and chunk length, replayed on the caller's stream.
+int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* out) {
+    auto it = ws->graphs.find(iters);
+    if (it != ws->graphs.end()) {
+        *out = it->second;
+        return NM_OK;
+    }
+    cudaGraph_t g = nullptr;
+    NM_CUDA_TRY(cudaStreamBeginCapture(ws->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < iters; ++i) launch_iteration(A, ws, ws->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(ws->cap_stream, &g);
+    if (e != cudaSuccess) return fail(NM_ERR_CUDA, "CG graph capture failed: %s", cudaGetErrorString(e));
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+        return fail(NM_ERR_CUDA, "CG graph instantiate failed: %s", cudaGetErrorString(e));
+    ws->graphs[iters] = ex;
+    *out = ex;
+    return NM_OK;
+}
+
+}  // namespace
+
+// Runs one CG solve on `s`; synchronises `s` before returning.
+int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, int guard,
+           nm_cg_result* res, cudaStream_t s) {
+    if (A->dtype != NM_F64) return fail(NM_ERR_TYPE, "cg: float64 matrices only");
+    if (A->nrows != A->ncols) return fail(NM_ERR_INVALID, "cg: matrix must be square");
+    if (!b || !x || !res) return fail(NM_ERR_INVALID, "cg: NULL argument");
+    std::lock_guard<std::mutex> lock(A->cg_mutex);
+    CgWorkspace* ws = nullptr;
+    int st = ensure_workspace(A, &ws);
+    if (st != NM_OK) return st;
+
+    CgState* h = ws->h_in;
+    std::memset(h, 0, sizeof(CgState));
+    h->b = b;
+    h->x = x;
+    h->tol = tol;
+    h->max_iter = max_iter;
+    h->guard = guard;
+    NM_CUDA_TRY(cudaMemcpyAsync(ws->st, h, sizeof(CgState), cudaMemcpyHostToDevice, s));
+    // r = b - A x0, p = r, ||b||, r.r, early exit.
+    st = launch_spmv(A, x, ws->Ap, s);
+    if (st != NM_OK) return st;
+    cg_init_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->Ap, ws->r, ws->p,
+                                                     ws->partials);
+    NM_CHECK_LAUNCH();
+
+    // Iterate in graph chunks of growing length; poll `done` in between.
+    int chunk = 8;
+    for (;;) {
+        NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+        NM_CUDA_TRY(cudaStreamSynchronize(s));
+        if (ws->h_out->done) break;
+        cudaGraphExec_t ex = nullptr;
+        st = chunk_graph(A, ws, chunk, &ex);
+        if (st != NM_OK) return st;
+        NM_CUDA_TRY(cudaGraphLaunch(ex, s));
+        if (chunk < 64) chunk *= 2;
+    }
+    const CgState& o = *ws->h_out;
+    if (o.status == kCgBreakdown)
+        return fail(NM_ERR_RUNTIME, "CG: p'Ap is near zero - A may not be SPD");
+    res->iters = o.iters;
+    res->final_res = o.final_res;
+    res->converged = o.converged;
+    return NM_OK;
+}
+
+}  // namespace nm
+
+extern "C" int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter,
+                           nm_cg_result* result, void* stream) {
+    nm::clear_error();
+    if (!A) return nm::fail(NM_ERR_INVALID, "nm_cg_local: NULL matrix");
+    return nm::cg_run(A, b, x, tol, max_iter, 0, result, static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,80 @@
+// cg.cuh -- device-resident CG state and the per-matrix CG workspace.
+#pragma once
+
+#include <map>
+
+#include "csr.cuh"
+
+namespace nm {
+
+// Scalars of one CG solve, resident in device memory.  The host writes the
+// inputs before a solve and reads the outputs after it; in between every
+// scalar step (alpha, beta, the stopping test) runs on the device, in the last
+// CTA of the reduction that produces its input.
+struct CgState {
+    // inputs
+    const double* b;
+    double* x;
+    double tol;
+    int32_t max_iter;
+    int32_t guard;  // 1: reject |p.Ap| < 1e-300 (cg_solve_distributed)
+    // scalars
+    double bnorm, rr, pAp, alpha, beta, final_res;
+    int32_t iter, done, converged, iters, status;
+    unsigned int counter;  // arrival counter of the last-CTA reductions
+};
+
+// Status codes written to CgState::status.
+constexpr int kCgOk = 0;
+constexpr int kCgBreakdown = 1;
+
+struct CgWorkspace {
+    int64_t n = 0;
+    double* r = nullptr;
+    double* p = nullptr;
+    double* Ap = nullptr;
+    double* partials = nullptr;
+    int partials_cap = 0;
+    CgState* st = nullptr;
+    CgState* h_in = nullptr;    // pinned staging of the inputs
+    CgState* h_out = nullptr;   // pinned landing of the outputs
+    int grid_spmv = 0, grid_vec = 0;
+    cudaStream_t cap_stream = nullptr;
+    std::map<int, cudaGraphExec_t> graphs;  // iterations per graph -> exec
+    ~CgWorkspace();
+};
+
+// Grid of the grid-stride vector kernels for n elements.
+int vec_grid(int64_t n);
+
+// Last-CTA grid reduction: every CTA passes K partial sums (valid in thread 0);
+// returns true on thread 0 of the CTA that arrives last, with the grid totals
+// summed in a fixed order (so results are bit-reproducible for a fixed grid).
+// The counter is reset for the next launch.  Call from all threads.
+template <int K>
+__device__ __forceinline__ bool grid_reduce_last(const double (&part)[K], double* partials,
+                                                 unsigned int* counter, double (&tot)[K],
+                                                 double* red) {
+    __shared__ bool am_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) partials[size_t(k) * gridDim.x + blockIdx.x] = part[k];
+        __threadfence();
+        const unsigned int prev = atomicAdd(counter, 1u);
+        am_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += kThreads)
+            s += __ldcg(partials + size_t(k) * gridDim.x + i);
+        tot[k] = block_sum(s, red);
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return threadIdx.x == 0;
+}
+
+}  // namespace nm

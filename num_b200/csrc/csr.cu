@@ -1,0 +1,286 @@
+// csr.cu -- device CSR matrix: upload, validation, row-block partition.
+//
+// Replaces CrsMatrixHandle (src/crs_matrix.hpp:37-73) and the global
+// rows-per-team pick of the reference custom kernel (src/spmv_kernel.hpp:102-109)
+// with a per-row-block partition computed once at upload.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "cg.cuh"
+#include "csr.cuh"
+
+namespace nm {
+
+int build_row_blocks(const int32_t* rp, int32_t nrows, int tile, int max_rows, int short_max,
+                     std::vector<int32_t>& blk, std::vector<int8_t>* bins) {
+    blk.clear();
+    blk.push_back(0);
+    if (bins) bins->assign(static_cast<size_t>(nrows), 0);
+    int32_t r = 0;
+    while (r < nrows) {
+        const int32_t len = rp[r + 1] - rp[r];
+        if (len > tile) {
+            if (bins) (*bins)[r] = 2;
+            ++r;
+        } else {
+            const int32_t start = r;
+            int64_t nz = 0;
+            while (r < nrows && r - start < max_rows) {
+                const int32_t l = rp[r + 1] - rp[r];
+                if (nz + l > tile) break;
+                if (bins) (*bins)[r] = static_cast<int8_t>(l <= short_max ? 0 : 1);
+                nz += l;
+                ++r;
+            }
+        }
+        blk.push_back(r);
+    }
+    return static_cast<int>(blk.size()) - 1;
+}
+
+namespace {
+
+size_t dtype_size(int dtype) {
+    switch (dtype) {
+        case NM_F64: return 8;
+        case NM_F32: return 4;
+        case NM_BF16: return 2;
+        default: return 0;
+    }
+}
+
+int normalise_tuning(nm_tuning& t) {
+    if (t.tile <= 0) t.tile = kDefaultTile;
+    if (t.max_rows <= 0) t.max_rows = kDefaultMaxRows;
+    if (t.short_max <= 0) t.short_max = kDefaultShortMax;
+    if (t.grid_mult < 0) t.grid_mult = 0;
+    if (t.tile != 1024 && t.tile != 2048 && t.tile != 4096)
+        return fail(NM_ERR_INVALID, "tuning: tile must be 1024, 2048 or 4096 (got %d)", t.tile);
+    if (t.max_rows > kThreads)
+        return fail(NM_ERR_INVALID, "tuning: max_rows must be <= %d (got %d)", kThreads,
+                    t.max_rows);
+    return NM_OK;
+}
+
+// Checks row_ptr (starts at 0, non-decreasing) and column bounds on the host.
+int validate_csr(const int32_t* rp, const int32_t* ci, int32_t nrows, int32_t ncols,
+                 const char* who) {
+    if (rp[0] != 0) return fail(NM_ERR_INVALID, "%s: row_ptr[0] must be 0 (got %d)", who, rp[0]);
+    for (int32_t i = 0; i < nrows; ++i)
+        if (rp[i + 1] < rp[i])
+            return fail(NM_ERR_INVALID, "%s: row_ptr decreases at row %d", who, i);
+    const int32_t nnz = rp[nrows];
+    if (nnz > INT32_MAX - 16384)
+        return fail(NM_ERR_INVALID, "%s: nnz %d exceeds the int32 offset range", who, nnz);
+    for (int32_t j = 0; j < nnz; ++j)
+        if (ci[j] < 0 || ci[j] >= ncols)
+            return fail(NM_ERR_INVALID, "%s: column index %d at nonzero %d outside [0, %d)", who,
+                        ci[j], j, ncols);
+    return NM_OK;
+}
+
+int upload(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals) {
+    const size_t es = dtype_size(A->dtype);
+    const int64_t nnz_pad = ((static_cast<int64_t>(A->nnz) + 3) & ~int64_t(3)) + 4;
+    NM_CUDA_TRY(cudaMalloc(&A->d_row_ptr, sizeof(int32_t) * (size_t(A->nrows) + 1)));
+    NM_CUDA_TRY(cudaMalloc(&A->d_col_idx, sizeof(int32_t) * size_t(nnz_pad)));
+    NM_CUDA_TRY(cudaMalloc(&A->d_values, es * size_t(nnz_pad)));
+    NM_CUDA_TRY(cudaMemcpy(A->d_row_ptr, rp, sizeof(int32_t) * (size_t(A->nrows) + 1),
+                           cudaMemcpyHostToDevice));
+    NM_CUDA_TRY(cudaMemset(A->d_col_idx, 0, sizeof(int32_t) * size_t(nnz_pad)));
+    NM_CUDA_TRY(cudaMemset(A->d_values, 0, es * size_t(nnz_pad)));
+    if (A->nnz > 0) {
+        NM_CUDA_TRY(cudaMemcpy(A->d_col_idx, ci, sizeof(int32_t) * size_t(A->nnz),
+                               cudaMemcpyHostToDevice));
+        NM_CUDA_TRY(cudaMemcpy(A->d_values, vals, es * size_t(A->nnz), cudaMemcpyHostToDevice));
+    }
+    return NM_OK;
+}
+
+int rebuild_blocks(nm_csr* A) {
+    std::vector<int32_t> blk;
+    A->nblk = build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
+                               A->tune.short_max, blk, nullptr);
+    if (A->d_blk) {
+        cudaFree(A->d_blk);
+        A->d_blk = nullptr;
+    }
+    NM_CUDA_TRY(cudaMalloc(&A->d_blk, sizeof(int32_t) * blk.size()));
+    NM_CUDA_TRY(cudaMemcpy(A->d_blk, blk.data(), sizeof(int32_t) * blk.size(),
+                           cudaMemcpyHostToDevice));
+    return NM_OK;
+}
+
+int finish_create(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals,
+                  nm_csr** out) {
+    int st = upload(A, rp, ci, vals);
+    if (st == NM_OK) {
+        A->h_row_ptr.assign(rp, rp + A->nrows + 1);
+        st = rebuild_blocks(A);
+    }
+    if (st != NM_OK) {
+        delete A;
+        return st;
+    }
+    *out = A;
+    return NM_OK;
+}
+
+}  // namespace
+
+int spmv_grid(const nm_csr* A, int ctas_per_sm) {
+    const int mult = A->tune.grid_mult > 0 ? A->tune.grid_mult : ctas_per_sm;
+    const int64_t g = int64_t(sm_count()) * mult;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, A->nblk)));
+}
+
+}  // namespace nm
+
+nm_csr::~nm_csr() {
+    cg.reset();
+    if (d_row_ptr) cudaFree(d_row_ptr);
+    if (d_col_idx) cudaFree(d_col_idx);
+    if (d_values) cudaFree(d_values);
+    if (d_blk) cudaFree(d_blk);
+}
+
+using nm::fail;
+
+extern "C" int nm_csr_create(const int32_t* row_ptr, const int32_t* col_idx, const void* values,
+                             int dtype, int32_t nrows, int32_t ncols, nm_csr** out) {
+    nm::clear_error();
+    if (!out) return fail(NM_ERR_INVALID, "nm_csr_create: out is NULL");
+    *out = nullptr;
+    if (nrows <= 0 || ncols <= 0)
+        return fail(NM_ERR_INVALID, "CrsMatrixHandle: non-positive dimensions");
+    if (nm::dtype_size(dtype) == 0) return fail(NM_ERR_TYPE, "nm_csr_create: unknown dtype %d", dtype);
+    if (!row_ptr || (row_ptr[nrows] > 0 && (!col_idx || !values)))
+        return fail(NM_ERR_INVALID, "nm_csr_create: NULL array");
+    int st = nm::validate_csr(row_ptr, col_idx, nrows, ncols, "nm_csr_create");
+    if (st != NM_OK) return st;
+    auto* A = new nm_csr();
+    cudaGetDevice(&A->device);
+    A->nrows = nrows;
+    A->ncols = ncols;
+    A->nnz = row_ptr[nrows];
+    A->dtype = dtype;
+    A->tune = nm_tuning{0, 0, 0, 0};
+    nm::normalise_tuning(A->tune);
+    return nm::finish_create(A, row_ptr, col_idx, values, out);
+}
+
+extern "C" int nm_csr_create_batched(int32_t count, const int32_t* nrows, const int32_t* ncols,
+                                     const int32_t* row_ptr, const int32_t* col_idx,
+                                     const void* values, int dtype, nm_csr** out) {
+    nm::clear_error();
+    if (!out) return fail(NM_ERR_INVALID, "nm_csr_create_batched: out is NULL");
+    *out = nullptr;
+    if (count <= 0) return fail(NM_ERR_INVALID, "nm_csr_create_batched: count must be > 0");
+    const size_t es = nm::dtype_size(dtype);
+    if (es == 0) return fail(NM_ERR_TYPE, "nm_csr_create_batched: unknown dtype %d", dtype);
+    std::vector<int32_t> row_off(count + 1, 0), col_off(count + 1, 0);
+    int64_t tot_rows = 0, tot_cols = 0, tot_nnz = 0, rp_pos = 0;
+    for (int32_t m = 0; m < count; ++m) {
+        if (nrows[m] <= 0 || ncols[m] <= 0)
+            return fail(NM_ERR_INVALID, "nm_csr_create_batched: matrix %d has non-positive dims", m);
+        const int32_t* rp = row_ptr + rp_pos;
+        char who[64];
+        snprintf(who, sizeof who, "nm_csr_create_batched[%d]", m);
+        int st = nm::validate_csr(rp, col_idx + tot_nnz, nrows[m], ncols[m], who);
+        if (st != NM_OK) return st;
+        tot_nnz += rp[nrows[m]];
+        rp_pos += nrows[m] + 1;
+        tot_rows += nrows[m];
+        tot_cols += ncols[m];
+        if (tot_rows > INT32_MAX - 1 || tot_cols > INT32_MAX - 1 || tot_nnz > INT32_MAX - 16384)
+            return fail(NM_ERR_INVALID, "nm_csr_create_batched: totals exceed the int32 range");
+        row_off[m + 1] = static_cast<int32_t>(tot_rows);
+        col_off[m + 1] = static_cast<int32_t>(tot_cols);
+    }
+    // Block-diagonal assembly: global row_ptr and column indices shifted by
+    // each matrix's column offset.
+    std::vector<int32_t> grp(static_cast<size_t>(tot_rows) + 1);
+    std::vector<int32_t> gci(static_cast<size_t>(tot_nnz));
+    grp[0] = 0;
+    int64_t nz_base = 0;
+    rp_pos = 0;
+    for (int32_t m = 0; m < count; ++m) {
+        const int32_t* rp = row_ptr + rp_pos;
+        for (int32_t i = 0; i < nrows[m]; ++i)
+            grp[row_off[m] + i + 1] = static_cast<int32_t>(nz_base + rp[i + 1]);
+        const int32_t nzm = rp[nrows[m]];
+        for (int32_t j = 0; j < nzm; ++j)
+            gci[nz_base + j] = col_idx[nz_base + j] + col_off[m];
+        nz_base += nzm;
+        rp_pos += nrows[m] + 1;
+    }
+    auto* A = new nm_csr();
+    cudaGetDevice(&A->device);
+    A->nrows = static_cast<int32_t>(tot_rows);
+    A->ncols = static_cast<int32_t>(tot_cols);
+    A->nnz = static_cast<int32_t>(tot_nnz);
+    A->dtype = dtype;
+    A->tune = nm_tuning{0, 0, 0, 0};
+    nm::normalise_tuning(A->tune);
+    A->batch_row_off = row_off;
+    A->batch_col_off = col_off;
+    return nm::finish_create(A, grp.data(), gci.data(), values, out);
+}
+
+extern "C" int nm_csr_destroy(nm_csr* A) {
+    nm::clear_error();
+    delete A;
+    return NM_OK;
+}
+
+extern "C" int nm_csr_info(const nm_csr* A, int32_t* nrows, int32_t* ncols, int32_t* nnz,
+                           int32_t* dtype, int32_t* nblocks) {
+    nm::clear_error();
+    if (!A) return fail(NM_ERR_INVALID, "nm_csr_info: NULL matrix");
+    if (nrows) *nrows = A->nrows;
+    if (ncols) *ncols = A->ncols;
+    if (nnz) *nnz = A->nnz;
+    if (dtype) *dtype = A->dtype;
+    if (nblocks) *nblocks = A->nblk;
+    return NM_OK;
+}
+
+extern "C" int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t) {
+    nm::clear_error();
+    if (!A || !t) return fail(NM_ERR_INVALID, "nm_csr_set_tuning: NULL argument");
+    nm_tuning nt = *t;
+    int st = nm::normalise_tuning(nt);
+    if (st != NM_OK) return st;
+    {
+        // Cached CG graphs hold the old partition; drop them.
+        std::lock_guard<std::mutex> lock(A->cg_mutex);
+        A->cg.reset();
+    }
+    A->tune = nt;
+    return nm::rebuild_blocks(A);
+}
+
+extern "C" int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t) {
+    nm::clear_error();
+    if (!A || !t) return fail(NM_ERR_INVALID, "nm_csr_get_tuning: NULL argument");
+    *t = A->tune;
+    return NM_OK;
+}
+
+extern "C" int nm_csr_row_blocks(const nm_csr* A, int32_t* blk, int32_t cap, int8_t* bins) {
+    nm::clear_error();
+    if (!A || !blk) return fail(NM_ERR_INVALID, "nm_csr_row_blocks: NULL argument");
+    std::vector<int32_t> b;
+    std::vector<int8_t> bn;
+    nm::build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
+                         A->tune.short_max, b, bins ? &bn : nullptr);
+    if (static_cast<int64_t>(b.size()) > cap)
+        return fail(NM_ERR_INVALID, "nm_csr_row_blocks: cap %d < %zu", cap, b.size());
+    // The host copy is what the device holds; read the device copy back to
+    // report exactly what the kernels use.
+    NM_CUDA_TRY(cudaMemcpy(blk, A->d_blk, sizeof(int32_t) * size_t(A->nblk + 1),
+                           cudaMemcpyDeviceToHost));
+    if (bins) std::memcpy(bins, bn.data(), bn.size());
+    return NM_OK;
+}

@@ -1,0 +1,76 @@
+// csr.cuh -- internal layout of a device CSR matrix.
+//
+// HBM layout (one cudaMalloc each, 256-byte aligned):
+//   row_ptr  int32[nrows + 1]
+//   col_idx  int32[nnz_pad]      nnz_pad = round_up(nnz, 4) + 4, pad = column 0
+//   values   V[nnz_pad]          pad = 0
+//   blk      int32[nblk + 1]     row-block boundaries (see build_row_blocks)
+// The padding lets every thread load 4 consecutive nonzeros with one 16-byte
+// access from a 4-aligned index without reading past the allocation.
+#pragma once
+
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace nm {
+
+struct CgWorkspace;  // cg.cu
+
+// Kernel-side view of a matrix.
+template <typename V>
+struct CsrView {
+    const int32_t* __restrict__ row_ptr;
+    const int32_t* __restrict__ col_idx;
+    const V* __restrict__ values;
+    const int32_t* __restrict__ blk;
+    int32_t nblk;
+    int32_t nrows;
+    int32_t short_max;
+};
+
+// Default row-block parameters.
+constexpr int kDefaultTile = 2048;
+constexpr int kDefaultMaxRows = kThreads;
+constexpr int kDefaultShortMax = 32;
+
+// Row-block partition rule, shared by the device library and restated by the
+// CPU oracle (oracle.c, or_row_blocks).  Returns nblk; blk gets nblk+1 entries.
+int build_row_blocks(const int32_t* row_ptr, int32_t nrows, int tile, int max_rows,
+                     int short_max, std::vector<int32_t>& blk, std::vector<int8_t>* bins);
+
+}  // namespace nm
+
+struct nm_csr {
+    int32_t nrows = 0, ncols = 0, nnz = 0;
+    int dtype = NM_F64;
+    int device = 0;
+    int32_t* d_row_ptr = nullptr;
+    int32_t* d_col_idx = nullptr;
+    void* d_values = nullptr;
+    int32_t* d_blk = nullptr;
+    int32_t nblk = 0;
+    nm_tuning tune{};
+    std::vector<int32_t> h_row_ptr;  // kept to rebuild the partition on retuning
+    // Many-matrix handles: per-matrix row / column offsets (count + 1 each).
+    std::vector<int32_t> batch_row_off, batch_col_off;
+    std::mutex cg_mutex;
+    std::unique_ptr<nm::CgWorkspace> cg;
+    ~nm_csr();
+
+    template <typename V>
+    nm::CsrView<V> view() const {
+        return nm::CsrView<V>{d_row_ptr, d_col_idx, static_cast<const V*>(d_values),
+                              d_blk,     nblk,      nrows,
+                              tune.short_max};
+    }
+};
+
+namespace nm {
+// Number of CTAs of a persistent SpMV-family grid for this matrix.
+int spmv_grid(const nm_csr* A, int ctas_per_sm);
+// Launches y = A*x on `stream` (dtype-dispatched).  Used by the API and CG.
+int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t stream);
+}  // namespace nm

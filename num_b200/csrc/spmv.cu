@@ -1,0 +1,148 @@
+// spmv.cu -- plain SpMV and multi-RHS SpMV kernels and their launchers.
+#include "spmv.cuh"
+
+namespace nm {
+
+template <typename V, typename X, typename A, int TILE>
+__global__ void __launch_bounds__(kThreads)
+    spmv_kernel(const CsrView<V> M, const X* __restrict__ x, X* __restrict__ y) {
+    __shared__ SpmvSmem<A, TILE> sm;
+    StoreEpi<X, A> epi{y};
+    for (int32_t b = blockIdx.x; b < M.nblk; b += gridDim.x)
+        spmv_block<V, X, A, TILE>(M, M.blk[b], M.blk[b + 1], x, sm, epi);
+}
+
+template <typename V, typename X, typename A>
+static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+    const CsrView<V> M = Am->view<V>();
+    // One CTA per row block unless a persistent grid was requested.
+    const int grid = Am->tune.grid_mult > 0 ? spmv_grid(Am, Am->tune.grid_mult) : Am->nblk;
+    switch (Am->tune.tile) {
+        case 1024: spmv_kernel<V, X, A, 1024><<<grid, kThreads, 0, s>>>(M, x, y); break;
+        case 2048: spmv_kernel<V, X, A, 2048><<<grid, kThreads, 0, s>>>(M, x, y); break;
+        case 4096: spmv_kernel<V, X, A, 4096><<<grid, kThreads, 0, s>>>(M, x, y); break;
+        default: return fail(NM_ERR_INVALID, "spmv: unsupported tile %d", Am->tune.tile);
+    }
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
+    switch (A->dtype) {
+        case NM_F64:
+            return launch_typed<double, double, double>(A, static_cast<const double*>(x),
+                                                        static_cast<double*>(y), s);
+        case NM_F32:
+            return launch_typed<float, float, float>(A, static_cast<const float*>(x),
+                                                     static_cast<float*>(y), s);
+        case NM_BF16:
+            return launch_typed<__nv_bfloat16, float, float>(A, static_cast<const float*>(x),
+                                                             static_cast<float*>(y), s);
+        default: return fail(NM_ERR_TYPE, "spmv: unknown dtype %d", A->dtype);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Multi-RHS SpMV  Y(nrows,k) = A * X(ncols,k), row-major.
+//
+// A group of TPR = 2^tpr_log2 consecutive lanes owns one row; lane g of the
+// group owns the columns g*VEC + m*TPR*VEC (m < MCH) of the current column
+// pass, VEC = 2 with 16-byte loads when k is even.  Each (row, column) sum
+// runs serially in CSR order with unfused multiply/add, i.e. exactly the
+// reference's per-(i,b) loop (src/batch_spmv_kernel.hpp:95-102).  The
+// matrix entries of a row are read once per column pass and broadcast to the
+// group; X rows are read as contiguous segments (coalesced).
+// ---------------------------------------------------------------------------
+constexpr int kBatchChunks = 4;
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads)
+    batch_spmv_kernel(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                      const double* __restrict__ vals, int32_t nrows, int32_t k, int tpr_log2,
+                      const double* __restrict__ X, double* __restrict__ Y) {
+    const int tpr = 1 << tpr_log2;
+    const int64_t gtid = int64_t(blockIdx.x) * kThreads + threadIdx.x;
+    const int64_t row = gtid >> tpr_log2;
+    const int g = static_cast<int>(gtid & (tpr - 1));
+    if (row >= nrows) return;
+    const int32_t s0 = rp[row], s1 = rp[row + 1];
+    const int pass_cols = tpr * VEC * kBatchChunks;
+    for (int c0 = 0; c0 < k; c0 += pass_cols) {
+        double acc[kBatchChunks][VEC];
+#pragma unroll
+        for (int m = 0; m < kBatchChunks; ++m)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) acc[m][e] = 0.0;
+        for (int32_t j = s0; j < s1; ++j) {
+            const double v = __ldg(vals + j);
+            const int64_t xrow = int64_t(__ldg(ci + j)) * k;
+#pragma unroll
+            for (int m = 0; m < kBatchChunks; ++m) {
+                const int c = c0 + (m * tpr + g) * VEC;
+                if (c < k) {
+                    if (VEC == 2) {
+                        const double2 xv = __ldg(reinterpret_cast<const double2*>(X + xrow + c));
+                        acc[m][0] = add_rn(acc[m][0], mul_rn(v, xv.x));
+                        acc[m][VEC - 1] = add_rn(acc[m][VEC - 1], mul_rn(v, xv.y));
+                    } else {
+                        acc[m][0] = add_rn(acc[m][0], mul_rn(v, __ldg(X + xrow + c)));
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < kBatchChunks; ++m) {
+            const int c = c0 + (m * tpr + g) * VEC;
+            if (c < k) {
+                if (VEC == 2) {
+                    *reinterpret_cast<double2*>(Y + row * k + c) =
+                        make_double2(acc[m][0], acc[m][VEC - 1]);
+                } else {
+                    Y[row * k + c] = acc[m][0];
+                }
+            }
+        }
+    }
+}
+
+static int launch_batch(const nm_csr* A, const double* X, double* Y, int32_t k, cudaStream_t s) {
+    const bool vec2 = (k % 2 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0) &&
+                      (reinterpret_cast<uintptr_t>(Y) % 16 == 0);
+    const int vec = vec2 ? 2 : 1;
+    const int groups = (k + vec - 1) / vec;  // lane-columns needed for one pass
+    int tpr_log2 = 0;
+    while ((1 << tpr_log2) < groups && tpr_log2 < 5) ++tpr_log2;
+    const int64_t threads = int64_t(A->nrows) << tpr_log2;
+    const int64_t grid = (threads + kThreads - 1) / kThreads;
+    if (grid > INT32_MAX) return fail(NM_ERR_INVALID, "batch_spmv: problem too large");
+    if (vec2)
+        batch_spmv_kernel<2><<<static_cast<int>(grid), kThreads, 0, s>>>(
+            A->d_row_ptr, A->d_col_idx, static_cast<const double*>(A->d_values), A->nrows, k,
+            tpr_log2, X, Y);
+    else
+        batch_spmv_kernel<1><<<static_cast<int>(grid), kThreads, 0, s>>>(
+            A->d_row_ptr, A->d_col_idx, static_cast<const double*>(A->d_values), A->nrows, k,
+            tpr_log2, X, Y);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+}  // namespace nm
+
+using nm::fail;
+
+extern "C" int nm_spmv(const nm_csr* A, const void* x, void* y, void* stream) {
+    nm::clear_error();
+    if (!A || !x || !y) return fail(NM_ERR_INVALID, "nm_spmv: NULL argument");
+    return nm::launch_spmv(A, x, y, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int nm_batch_spmv(const nm_csr* A, const double* X, double* Y, int32_t k,
+                             void* stream) {
+    nm::clear_error();
+    if (!A || !X || !Y) return fail(NM_ERR_INVALID, "nm_batch_spmv: NULL argument");
+    if (A->dtype != NM_F64) return fail(NM_ERR_TYPE, "batch_spmv: float64 matrices only");
+    if (k < 0) return fail(NM_ERR_INVALID, "batch_spmv: k must be >= 0");
+    if (k == 0) return NM_OK;  // launch_batch_spmv returns early for k == 0
+    return nm::launch_batch(A, X, Y, k, static_cast<cudaStream_t>(stream));
+}

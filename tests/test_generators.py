@@ -1,0 +1,79 @@
+"""The workload generators: identical to the reference's generators where it
+has them (hashes recorded from the reference by tests/golden/make_golden.py),
+and the stated properties of the synthetic workloads otherwise."""
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from num_b200 import generators as gen
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+REF = json.loads((GOLDEN / "ref_generators.json").read_text())
+
+
+@pytest.mark.parametrize("key", sorted(REF))
+def test_matches_reference_generators(key):
+    kind, L = key.rsplit("_", 1)
+    A = (gen.laplacian_2d if kind == "laplacian_2d" else gen.laplacian_3d)(int(L))
+    ref = REF[key]
+    assert A.nnz == ref["nnz"]
+    assert sha(A.row_ptr) == ref["indptr"]
+    assert sha(A.col_idx) == ref["indices"]
+    assert sha(A.values) == ref["data"]
+
+
+def test_power_law_properties():
+    A = gen.power_law(200_000, seed=11)
+    lens = np.diff(A.row_ptr)
+    assert lens.min() >= 1 and lens.max() <= 2048
+    assert 14.0 < lens.mean() < 18.0
+    for i in np.random.default_rng(0).integers(0, A.nrows, 2000):
+        c = A.col_idx[A.row_ptr[i]:A.row_ptr[i + 1]]
+        assert np.all(np.diff(c) > 0)  # ascending, no repeats
+    assert abs(A.values.mean()) < 0.01 and abs(A.values.std() - 1) < 0.01
+
+
+def test_banded_batch_properties():
+    mats, xs = gen.banded_batch(64, seed=2)
+    for A, x in zip(mats, xs):
+        assert 32 <= A.nrows <= 4096 and x.shape == (A.nrows,)
+        S = A.to_scipy()
+        assert (S - S.T).nnz == 0                       # symmetric
+        d = S.diagonal()
+        off = np.asarray(abs(S).sum(axis=1)).ravel() - np.abs(d)
+        assert np.allclose(d, 1.05 * off)                # diagonal = 1.05 x row sum
+        assert np.all(S.data[S.indices != np.repeat(np.arange(A.nrows), np.diff(A.row_ptr))] <= 0)
+        for i in range(0, A.nrows, 7):
+            assert np.all(np.diff(A.col_idx[A.row_ptr[i]:A.row_ptr[i + 1]]) > 0)
+
+
+def test_varcoef_poisson_properties():
+    A, b = gen.varcoef_poisson_3d(16, seed=3)
+    n = 16 ** 3
+    assert A.nrows == n and A.nnz == 7 * n - 6 * 16 * 16 and b.shape == (n,)
+    S = A.to_scipy()
+    assert abs(S - S.T).max() == 0
+    off = np.asarray(abs(S).sum(axis=1)).ravel() - S.diagonal()
+    # weakly diagonally dominant everywhere (equality inside), strictly at the
+    # Dirichlet boundary, irreducible => SPD
+    assert np.all(S.diagonal() >= off * (1 - 1e-15)) and np.any(S.diagonal() > off * 1.01)
+
+
+def test_c4_nnz_matches_stencil_count():
+    # 128^3: n = 2,097,152 and 7n - 6*128^2 = 14,581,760 nonzeros
+    L = 128
+    assert 7 * L ** 3 - 6 * L * L == 14_581_760
+
+
+def test_spmv_bytes_formula():
+    # 3-D 160^3 FP64: 424.14 MB per SpMV
+    A_nnz, n = 28_518_400, 4_096_000
+    assert gen.spmv_bytes(A_nnz, n, n) == 12 * A_nnz + 4 * (n + 1) + 16 * n
+    assert abs(gen.spmv_bytes(A_nnz, n, n) / 1e6 - 424.14) < 0.01

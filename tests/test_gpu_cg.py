@@ -1,0 +1,234 @@
+"""GPU parity of CG, multi-RHS SpMV and the vector ops against the oracle.
+
+CG bar (from the path's specification): iteration counts identical to the
+oracle's restatement of cg_solve_local, the same convergence outcome, and the
+same relative residual to within reduction-order noise; every known answer of
+the reference's tests/test_cg.cpp holds through the drop-in API."""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from num_b200 import generators as gen
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+
+def _cg(kspmv, A, b, x0=None, tol=1e-10, max_iter=1000):
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    bt = _dev(b)
+    xt = _dev(np.zeros(A.nrows) if x0 is None else x0)
+    info = kspmv.cg_solve_local(M, bt, xt, tol=tol, max_iter=max_iter)
+    return info, xt.cpu().numpy()
+
+
+def test_identity(kspmv):
+    b = np.arange(1, 51, dtype=np.float64)
+    info, x = _cg(kspmv, gen.diagonal(np.ones(50)), b, tol=1e-12, max_iter=200)
+    assert info["converged"] and info["iters"] <= 2
+    assert np.linalg.norm(x - b) / np.linalg.norm(b) < 1e-10
+
+
+def test_2x2(kspmv):
+    A = gen.Csr(np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32),
+                np.array([4.0, 1.0, 1.0, 3.0]), 2, 2)
+    info, x = _cg(kspmv, A, [1.0, 2.0], tol=1e-14, max_iter=100)
+    ex = np.array([1 / 11, 7 / 11])
+    assert info["converged"] and info["iters"] <= 2
+    assert np.linalg.norm(x - ex) / np.linalg.norm(ex) < 1e-10
+
+
+def test_diagonal(kspmv):
+    d = np.arange(1, 101, dtype=np.float64)
+    info, x = _cg(kspmv, gen.diagonal(d), np.ones(100), tol=1e-12, max_iter=5000)
+    assert info["converged"] and np.linalg.norm(x - 1 / d) / np.linalg.norm(1 / d) < 1e-8
+
+
+def test_laplacian_1d(kspmv):
+    info, _ = _cg(kspmv, gen.laplacian_1d(50), np.ones(50), tol=1e-10, max_iter=500)
+    assert info["converged"] and info["residual"] < 1e-10 and info["iters"] > 0
+
+
+def test_zero_rhs(kspmv):
+    info, x = _cg(kspmv, gen.laplacian_1d(20), np.zeros(20), tol=1e-10, max_iter=100)
+    assert info == {"iters": 0, "residual": 0.0, "converged": True}
+    assert np.array_equal(x, np.zeros(20))
+
+
+def test_manufactured_sin(kspmv):
+    N = 500
+    xe = np.sin(np.pi * (np.arange(N) + 1.0) / (N + 1.0))
+    b = 2.0 * xe
+    b[1:] -= xe[:-1]
+    b[:-1] -= xe[1:]
+    info, x = _cg(kspmv, gen.laplacian_1d(N), b, tol=1e-10, max_iter=2000)
+    assert info["converged"] and np.linalg.norm(x - xe) / np.linalg.norm(xe) < 1e-8
+
+
+@pytest.mark.parametrize("max_iter", [5, 1, 0, -2])
+def test_max_iter(kspmv, oracle, max_iter):
+    A = gen.laplacian_1d(50)
+    info, x = _cg(kspmv, A, np.ones(50), tol=1e-14, max_iter=max_iter)
+    oinfo, ox = oracle.cg_local(A.row_ptr, A.col_idx, A.values, np.ones(50), tol=1e-14,
+                                max_iter=max_iter)
+    assert info["iters"] == oinfo["iters"] == max_iter and not info["converged"]
+    assert abs(info["residual"] - oinfo["residual"]) <= 1e-12 * oinfo["residual"]
+    assert np.allclose(x, ox, rtol=1e-12, atol=1e-14)
+
+
+def test_repeated_solves_bit_identical(kspmv):
+    A = gen.laplacian_1d(30)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, 30, 30)
+    b = _dev(np.ones(30))
+    sols = []
+    for _ in range(3):
+        x = torch.zeros(30, dtype=torch.float64, device="cuda")
+        kspmv.cg_solve_local(M, b, x, tol=1e-12, max_iter=500)
+        sols.append(x.cpu().numpy())
+    assert np.array_equal(sols[0], sols[1]) and np.array_equal(sols[0], sols[2])
+
+
+def test_c1_iteration_parity(kspmv, oracle):
+    # 256^2 Laplacian, b = A*ones, x0 = 0, tol 1e-8: 454 iterations, like the
+    # oracle and SciPy; true residual < 1e-8.
+    probe = json.loads((GOLDEN / "c1_probe.json").read_text())
+    A = gen.laplacian_2d(256)
+    b = oracle.spmv(A.row_ptr, A.col_idx, A.values, np.ones(A.ncols))
+    info, x = _cg(kspmv, A, b, tol=1e-8, max_iter=5000)
+    oinfo, ox = oracle.cg_local(A.row_ptr, A.col_idx, A.values, b, tol=1e-8, max_iter=5000)
+    assert info["iters"] == oinfo["iters"] == probe["scipy_cg_iters"] == 454
+    assert info["converged"]
+    assert abs(info["residual"] - oinfo["residual"]) < 1e-6 * oinfo["residual"]
+    true_rel = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
+    assert true_rel < 1e-8
+    assert np.linalg.norm(x - ox) / np.linalg.norm(ox) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["laplacian_2d", "laplacian_3d", "random_sparse"])
+def test_vs_scipy_cg(kspmv, oracle, name):
+    # test_accuracy.py:160-195: solution vs spla.cg(rtol=1e-12), rel < 1e-6
+    p = np.load(GOLDEN / "scipy_pins.npz")
+    rp, ci, v = p[f"{name}__indptr"], p[f"{name}__indices"], p[f"{name}__data"]
+    n = rp.shape[0] - 1
+    A = gen.Csr(rp, ci, v, n, n)
+    info, x = _cg(kspmv, A, np.ones(n), tol=1e-10, max_iter=5000)
+    oinfo, _ = oracle.cg_local(rp, ci, v, np.ones(n), tol=1e-10, max_iter=5000)
+    assert info["converged"] and info["iters"] == oinfo["iters"]
+    ref = p[f"{name}__cg_x"]
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-6
+
+
+def test_nonzero_initial_guess(kspmv, oracle):
+    A = gen.laplacian_3d(20)
+    rng = np.random.default_rng(8)
+    b, x0 = rng.standard_normal(A.nrows), rng.standard_normal(A.nrows)
+    info, x = _cg(kspmv, A, b, x0=x0, tol=1e-9, max_iter=3000)
+    oinfo, ox = oracle.cg_local(A.row_ptr, A.col_idx, A.values, b, x0=x0, tol=1e-9, max_iter=3000)
+    assert info["iters"] == oinfo["iters"] and info["converged"]
+    assert np.linalg.norm(x - ox) / np.linalg.norm(ox) < 1e-8
+
+
+def test_singular_matrix_runs_to_max_iter(kspmv, oracle):
+    # cg_solve_local has no breakdown guard: p.Ap = 0 gives NaN and the loop
+    # runs to max_iter, returning converged=False.
+    A = gen.Csr(np.arange(5, dtype=np.int32), np.arange(4, dtype=np.int32), np.zeros(4), 4, 4)
+    info, _ = _cg(kspmv, A, np.ones(4), max_iter=7)
+    oinfo, _ = oracle.cg_local(A.row_ptr, A.col_idx, A.values, np.ones(4), max_iter=7)
+    assert info["iters"] == oinfo["iters"] == 7 and not info["converged"]
+    assert np.isnan(info["residual"]) and np.isnan(oinfo["residual"])
+
+
+def test_dist_single_rank_and_guard(kspmv, oracle):
+    A = gen.laplacian_2d(40)
+    D = kspmv.distribute_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    assert (D.global_nrows, D.local_row_start, D.local_row_end) == (1600, 0, 1600)
+    x = np.random.default_rng(3).standard_normal(A.nrows)
+    y = torch.empty(A.nrows, dtype=torch.float64, device="cuda")
+    kspmv.dist_spmv(D, _dev(x), y)
+    assert np.array_equal(y.cpu().numpy(), oracle.spmv(A.row_ptr, A.col_idx, A.values, x))
+    b = np.ones(A.nrows)
+    xt = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
+    info = kspmv.cg_solve(D, _dev(b), xt, tol=1e-10, max_iter=1000)
+    oinfo, _ = oracle.cg_local(A.row_ptr, A.col_idx, A.values, b, tol=1e-10, max_iter=1000)
+    assert info["iters"] == oinfo["iters"] and info["converged"]
+    Z = gen.Csr(np.arange(4, dtype=np.int32), np.arange(3, dtype=np.int32), np.zeros(3), 3, 3)
+    DZ = kspmv.distribute_csr(Z.row_ptr, Z.col_idx, Z.values, 3, 3)
+    with pytest.raises(RuntimeError, match="near zero"):
+        kspmv.cg_solve(DZ, _dev(np.ones(3)), torch.zeros(3, dtype=torch.float64, device="cuda"))
+
+
+# ---- multi-RHS SpMV -------------------------------------------------------------
+
+def test_batch_identity_columns(kspmv):
+    # tests/test_spmv_kernel.cpp:134-159
+    A = gen.tridiag4()
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, 4, 4)
+    X = _dev(np.eye(4))
+    Y = torch.empty(4, 4, dtype=torch.float64, device="cuda")
+    kspmv.batch_spmv(M, X, Y)
+    assert np.array_equal(Y.cpu().numpy(), A.to_scipy().toarray())
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 31, 32, 33, 64, 100, 300])
+def test_batch_bit_exact(kspmv, oracle, k):
+    A = gen.power_law(5000, seed=k)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    X = np.random.default_rng(k).standard_normal((A.ncols, k))
+    Y = torch.empty(A.nrows, k, dtype=torch.float64, device="cuda")
+    kspmv.batch_spmv(M, _dev(X), Y)
+    assert np.array_equal(Y.cpu().numpy(), oracle.batch_spmv(A.row_ptr, A.col_idx, A.values, X))
+
+
+def test_batch_errors(kspmv):
+    A = gen.tridiag4()
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, 4, 4)
+    with pytest.raises(ValueError, match=r"X.shape\[0\]"):
+        kspmv.batch_spmv(M, _dev(np.zeros((5, 2))), _dev(np.zeros((4, 2))))
+    with pytest.raises(ValueError, match="Y must be"):
+        kspmv.batch_spmv(M, _dev(np.zeros((4, 2))), _dev(np.zeros((4, 3))))
+
+
+# ---- vector ops through the C ABI ----------------------------------------------------
+
+def test_vector_ops_bit_exact(nmlib, kspmv, oracle):
+    rng = np.random.default_rng(12)
+    n = 1_000_003
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    xt, yt, zt = _dev(x), _dev(y), torch.empty(n, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert nmlib.nm_axpy(n, 0.37, xt.data_ptr(), yt.data_ptr(), zt.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(zt.cpu().numpy(), oracle.axpy(0.37, x, y))
+    assert nmlib.nm_axpy2(n, 0.37, xt.data_ptr(), -1.9, yt.data_ptr(), zt.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(zt.cpu().numpy(), oracle.axpy2(0.37, x, -1.9, y))
+    # aliasing z == x (as CG's x = alpha*p + x)
+    assert nmlib.nm_axpy(n, 2.0, yt.data_ptr(), xt.data_ptr(), xt.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(xt.cpu().numpy(), oracle.axpy(2.0, y, x))
+    d1, d2 = C.c_double(), C.c_double()
+    assert nmlib.nm_dot(n, xt.data_ptr(), yt.data_ptr(), C.byref(d1), s) == 0
+    assert nmlib.nm_dot(n, xt.data_ptr(), yt.data_ptr(), C.byref(d2), s) == 0
+    xn = xt.cpu().numpy()
+    ref = oracle.dot(xn, y)
+    assert d1.value == d2.value  # deterministic
+    assert abs(d1.value - ref) <= 1e-12 * float(np.abs(xn) @ np.abs(y))
+    nrm = C.c_double()
+    assert nmlib.nm_norm2(n, yt.data_ptr(), C.byref(nrm), s) == 0
+    assert abs(nrm.value - oracle.norm2(y)) < 1e-13 * oracle.norm2(y)
+    assert nmlib.nm_fill(n, 2.5, zt.data_ptr(), s) == 0
+    assert nmlib.nm_scale(n, -2.0, zt.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert np.all(zt.cpu().numpy() == -5.0)
+    assert nmlib.nm_copy(n, yt.data_ptr(), zt.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(zt.cpu().numpy(), y)
+    zero = C.c_double(7.0)
+    assert nmlib.nm_dot(0, None, None, C.byref(zero), s) == 0 and zero.value == 0.0
