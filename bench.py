@@ -170,6 +170,8 @@ def run_ours(args, rank, world, local_rank):
     desc, precision = WORKLOADS[args.workload]
     A, x = make_workload(args.workload)
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols, precision=precision)
+    tuned = kspmv.tune(M, tile=args.tile, short_max=args.short_max, stages=args.stages,
+                       grid_mult=args.grid_mult)
     dt = torch.float64 if precision == "fp64" else torch.float32
     xd = torch.tensor(x, dtype=dt, device=dev)
     yd = torch.empty(A.nrows, dtype=dt, device=dev)
@@ -263,6 +265,7 @@ def run_ours(args, rank, world, local_rank):
             "bytes_formula": "12*nnz + 4*(n+1) + 8*ncols + 8*nrows (fp64)",
             "l2": "inputs larger than L2 (no flush): %.1f MB per step > 126 MB" % (nbytes / 1e6),
             "parallelism": f"replicas x{world}",
+            "tuning": tuned,
         },
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -398,6 +401,10 @@ def main():
     ap.add_argument("--workload", default="spmv_c2a", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--tile", type=int, default=0, help="row-block tile (0: library default)")
+    ap.add_argument("--stages", type=int, default=0, help="TMA pipeline depth (0: default)")
+    ap.add_argument("--short-max", type=int, default=0)
+    ap.add_argument("--grid-mult", type=int, default=-1)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -51,6 +51,7 @@ typedef struct {
     int32_t max_rows;   /* max rows of a block (<= 256)                             */
     int32_t short_max;  /* rows with <= short_max nonzeros: one thread; else a warp */
     int32_t grid_mult;  /* CTAs launched per SM by the persistent SpMV grid (0: auto) */
+    int32_t stages;     /* TMA pipeline depth of the SpMV kernels: 2 or 3             */
 } nm_tuning;
 
 typedef struct nm_csr nm_csr;    /* device CSR matrix (CrsMatrixHandle)   */
@@ -71,6 +72,12 @@ int nm_init(int device_id, int32_t* rank, int32_t* size);
 
 /* finalize() (src/bindings.cpp:68-70): releases cached workspaces. */
 int nm_finalize(void);
+
+/* Reads and clears the current device's error word.  Kernels that stage data
+ * with TMA wait on mbarriers with a time limit (~2 s); one that gives up sets
+ * the word and exits instead of hanging.  Call after synchronising the stream;
+ * returns NM_ERR_RUNTIME if any kernel gave up since the last call. */
+int nm_check_device_errors(void);
 
 /* ---- CSR matrix ------------------------------------------------------------ */
 
@@ -103,8 +110,10 @@ int nm_csr_info(const nm_csr* A, int32_t* nrows, int32_t* ncols, int32_t* nnz,
                 int32_t* dtype, int32_t* nblocks);
 
 /* Replaces pick_rows_per_team (src/spmv_kernel.hpp:102-109): sets the
- * row-block partition parameters and rebuilds the partition.  Fields <= 0
- * keep their defaults (2048, 256, 32, auto). */
+ * row-block partition parameters and rebuilds the partition.  tile,
+ * max_rows, short_max and stages <= 0 (grid_mult < 0) keep their current
+ * values; grid_mult 0 selects the automatic grid.  Defaults: 2048, 256, 32,
+ * 0, 2. */
 int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t);
 int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t);
 

@@ -28,7 +28,7 @@ class CgResult(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tile", C.c_int32), ("max_rows", C.c_int32), ("short_max", C.c_int32),
-                ("grid_mult", C.c_int32)]
+                ("grid_mult", C.c_int32), ("stages", C.c_int32)]
 
 
 # name -> (argtypes); every function returns int (nm_status) unless noted.
@@ -37,6 +37,7 @@ _SIGNATURES = {
     "nm_version": ([], C.c_char_p),
     "nm_init": ([C.c_int, P_i32, P_i32], C.c_int),
     "nm_finalize": ([], C.c_int),
+    "nm_check_device_errors": ([], C.c_int),
     "nm_csr_create": ([vp, vp, vp, C.c_int, i32, i32, C.POINTER(vp)], C.c_int),
     "nm_csr_create_batched": ([i32, vp, vp, vp, vp, vp, C.c_int, C.POINTER(vp)], C.c_int),
     "nm_csr_destroy": ([vp], C.c_int),

@@ -1,4 +1,5 @@
 // api.cu -- error reporting, device context, host-only helpers.
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -41,6 +42,59 @@ int sm_count() {
 
 void release_dot_scratch();  // vec.cu
 
+namespace {
+std::mutex g_kern_mu;
+std::map<std::pair<const void*, int>, int> g_kern_occ;  // (kernel, device) -> CTAs per SM
+}  // namespace
+
+int prepare_kernel(const void* fn, size_t smem, int* ctas_per_sm) {
+    int dev = 0;
+    NM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(g_kern_mu);
+    auto key = std::make_pair(fn, dev);
+    auto it = g_kern_occ.find(key);
+    if (it != g_kern_occ.end()) {
+        *ctas_per_sm = it->second;
+        return NM_OK;
+    }
+    if (smem > 48 * 1024)
+        NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+    NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+    int occ = 0;
+    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem));
+    if (occ < 1) return fail(NM_ERR_CUDA, "kernel does not fit on an SM (%zu B shared)", smem);
+    g_kern_occ[key] = occ;
+    *ctas_per_sm = occ;
+    return NM_OK;
+}
+
+namespace {
+std::mutex g_err_mu;
+std::unordered_map<int, std::pair<unsigned int*, unsigned int*>> g_err;  // dev -> (host, device)
+}  // namespace
+
+unsigned int* device_error_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> g(g_err_mu);
+    auto it = g_err.find(dev);
+    if (it != g_err.end()) return it->second.second;
+    unsigned int* h = nullptr;
+    unsigned int* d = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&h), sizeof(unsigned int), cudaHostAllocMapped) !=
+        cudaSuccess)
+        return nullptr;
+    *h = 0u;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&d), h, 0) != cudaSuccess) {
+        cudaFreeHost(h);
+        return nullptr;
+    }
+    g_err[dev] = {h, d};
+    return d;
+}
+
 }  // namespace nm
 
 using nm::fail;
@@ -62,6 +116,25 @@ extern "C" int nm_init(int device_id, int32_t* rank, int32_t* size) {
     return NM_OK;
 }
 
+extern "C" int nm_check_device_errors(void) {
+    nm::clear_error();
+    int dev = 0;
+    NM_CUDA_TRY(cudaGetDevice(&dev));
+    unsigned int code = 0;
+    {
+        std::lock_guard<std::mutex> g(nm::g_err_mu);
+        auto it = nm::g_err.find(dev);
+        if (it == nm::g_err.end()) return NM_OK;
+        code = *reinterpret_cast<volatile unsigned int*>(it->second.first);
+        *reinterpret_cast<volatile unsigned int*>(it->second.first) = 0u;
+    }
+    if (code & nm::kErrWaitTimeout)
+        return fail(NM_ERR_RUNTIME,
+                    "a kernel gave up a bounded wait for its TMA copies; results are invalid");
+    if (code) return fail(NM_ERR_RUNTIME, "device error code 0x%x", code);
+    return NM_OK;
+}
+
 extern "C" int nm_finalize(void) {
     nm::clear_error();
     nm::release_dot_scratch();
@@ -75,7 +148,7 @@ extern "C" int nm_row_blocks_host(const int32_t* row_ptr, int32_t nrows, const n
     nm::clear_error();
     if (!row_ptr || !blk || !nblk || nrows < 0)
         return fail(NM_ERR_INVALID, "nm_row_blocks_host: bad argument");
-    nm_tuning tt = t ? *t : nm_tuning{0, 0, 0, 0};
+    nm_tuning tt = t ? *t : nm_tuning{0, 0, 0, 0, 0};
     if (tt.tile <= 0) tt.tile = nm::kDefaultTile;
     if (tt.max_rows <= 0) tt.max_rows = nm::kDefaultMaxRows;
     if (tt.short_max <= 0) tt.short_max = nm::kDefaultShortMax;

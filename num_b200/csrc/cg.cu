@@ -73,15 +73,21 @@ struct PApEpi {
     }
 };
 
-template <int TILE>
+template <int TILE, int STAGES>
 __global__ void __launch_bounds__(kThreads)
     cg_spmv_pap_kernel(const CsrView<double> M, CgState* st, const double* __restrict__ p,
-                       double* __restrict__ Ap, double* partials) {
+                       double* __restrict__ Ap, double* partials, unsigned int* err) {
     if (__ldcg(&st->done)) return;
-    __shared__ SpmvSmem<double, TILE> sm;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, TILE, STAGES>*>(smem_raw);
     PApEpi epi{Ap, p, 0.0};
-    for (int32_t b = blockIdx.x; b < M.nblk; b += gridDim.x)
-        spmv_block<double, double, double, TILE>(M, M.blk[b], M.blk[b + 1], p, sm, epi);
+    const bool ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
+    if (!ok && threadIdx.x == 0) {
+        // A bounded wait gave up: end the solve; every CTA still takes part in
+        // the reduction below so the arrival counter stays consistent.
+        atomicExch(&st->status, kCgDeviceError);
+        atomicExch(&st->done, 1);
+    }
     double part[1] = {block_sum(epi.dot, sm.red)};
     double tot[1];
     if (grid_reduce_last<1>(part, partials, &st->counter, tot, sm.red)) {
@@ -158,6 +164,17 @@ CgWorkspace::~CgWorkspace() {
 
 namespace {
 
+template <int TILE, int STAGES>
+int prepare_cg_spmv(int* occ) {
+    return prepare_kernel(reinterpret_cast<const void*>(cg_spmv_pap_kernel<TILE, STAGES>),
+                          spmv_smem_bytes<double, double, TILE, STAGES>(), occ);
+}
+
+template <int TILE>
+int prepare_cg_spmv_s(int stages, int* occ) {
+    return stages == 3 ? prepare_cg_spmv<TILE, 3>(occ) : prepare_cg_spmv<TILE, 2>(occ);
+}
+
 int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     if (A->cg) {
         *out = A->cg.get();
@@ -166,38 +183,59 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     auto ws = std::make_unique<CgWorkspace>();
     const int64_t n = A->nrows;
     ws->n = n;
-    ws->grid_spmv = spmv_grid(A, 8);
     ws->grid_vec = vec_grid(n);
-    ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
     NM_CUDA_TRY(cudaMalloc(&ws->r, sizeof(double) * size_t(n)));
     NM_CUDA_TRY(cudaMalloc(&ws->p, sizeof(double) * size_t(n)));
     NM_CUDA_TRY(cudaMalloc(&ws->Ap, sizeof(double) * size_t(n)));
-    NM_CUDA_TRY(cudaMalloc(&ws->partials, sizeof(double) * size_t(ws->partials_cap)));
     NM_CUDA_TRY(cudaMalloc(&ws->st, sizeof(CgState)));
     NM_CUDA_TRY(cudaMemset(ws->st, 0, sizeof(CgState)));
     NM_CUDA_TRY(cudaMallocHost(&ws->h_in, sizeof(CgState)));
     NM_CUDA_TRY(cudaMallocHost(&ws->h_out, sizeof(CgState)));
     NM_CUDA_TRY(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
+    // Load the iteration kernels and set their shared-memory attributes now
+    // (lazy module loading), not during graph capture.
+    cudaFuncAttributes fa;
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, cg_update_xr_kernel));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, cg_update_p_kernel));
+    int occ = 0, st = NM_OK;
+    switch (A->tune.tile) {
+        case 1024: st = prepare_cg_spmv_s<1024>(A->tune.stages, &occ); break;
+        case 4096: st = prepare_cg_spmv_s<4096>(A->tune.stages, &occ); break;
+        default: st = prepare_cg_spmv_s<2048>(A->tune.stages, &occ); break;
+    }
+    if (st != NM_OK) return st;
+    ws->grid_spmv = spmv_grid(A, occ);
+    ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
+    NM_CUDA_TRY(cudaMalloc(&ws->partials, sizeof(double) * size_t(ws->partials_cap)));
+    ws->err = device_error_word();
+    if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
     A->cg = std::move(ws);
     *out = A->cg.get();
     return NM_OK;
 }
 
-template <int TILE>
+template <int TILE, int STAGES>
 void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
     const CsrView<double> M = A->view<double>();
-    cg_spmv_pap_kernel<TILE><<<ws->grid_spmv, kThreads, 0, s>>>(M, ws->st, ws->p, ws->Ap,
-                                                                 ws->partials);
+    cg_spmv_pap_kernel<TILE, STAGES>
+        <<<ws->grid_spmv, kThreads, spmv_smem_bytes<double, double, TILE, STAGES>(), s>>>(
+            M, ws->st, ws->p, ws->Ap, ws->partials, ws->err);
     cg_update_xr_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->p, ws->Ap, ws->r,
                                                           ws->partials);
     cg_update_p_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->p, ws->r);
 }
 
+template <int TILE>
+void launch_iteration_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    if (A->tune.stages == 3) launch_iteration_t<TILE, 3>(A, ws, s);
+    else launch_iteration_t<TILE, 2>(A, ws, s);
+}
+
 void launch_iteration(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
     switch (A->tune.tile) {
-        case 1024: launch_iteration_t<1024>(A, ws, s); break;
-        case 4096: launch_iteration_t<4096>(A, ws, s); break;
-        default: launch_iteration_t<2048>(A, ws, s); break;
+        case 1024: launch_iteration_s<1024>(A, ws, s); break;
+        case 4096: launch_iteration_s<4096>(A, ws, s); break;
+        default: launch_iteration_s<2048>(A, ws, s); break;
     }
 }
 
@@ -265,6 +303,10 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
         if (chunk < 64) chunk *= 2;
     }
     const CgState& o = *ws->h_out;
+    st = nm_check_device_errors();
+    if (st != NM_OK) return st;
+    if (o.status == kCgDeviceError)
+        return fail(NM_ERR_RUNTIME, "cg: a device wait gave up; the solve was abandoned");
     if (o.status == kCgBreakdown)
         return fail(NM_ERR_RUNTIME, "CG: p'Ap is near zero - A may not be SPD");
     res->iters = o.iters;

@@ -27,6 +27,7 @@ struct CgState {
 // Status codes written to CgState::status.
 constexpr int kCgOk = 0;
 constexpr int kCgBreakdown = 1;
+constexpr int kCgDeviceError = 2;
 
 struct CgWorkspace {
     int64_t n = 0;
@@ -39,6 +40,7 @@ struct CgWorkspace {
     CgState* h_in = nullptr;    // pinned staging of the inputs
     CgState* h_out = nullptr;   // pinned landing of the outputs
     int grid_spmv = 0, grid_vec = 0;
+    unsigned int* err = nullptr;  // device error word (not owned)
     cudaStream_t cap_stream = nullptr;
     std::map<int, cudaGraphExec_t> graphs;  // iterations per graph -> exec
     ~CgWorkspace();

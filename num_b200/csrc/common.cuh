@@ -24,6 +24,19 @@ void clear_error();
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Device-visible error word of the current device (mapped pinned host memory,
+// zero until a kernel reports a failed bounded wait).  Kernels OR codes into
+// it; nm_check_device_errors() reads and clears it on the host.
+unsigned int* device_error_word();
+
+// Opts kernel `fn` into `smem` bytes of dynamic shared memory and the
+// maximum shared-memory carveout on the current device (once per device) and
+// returns how many CTAs of kThreads threads fit on one SM.
+int prepare_kernel(const void* fn, size_t smem, int* ctas_per_sm);
+
+// Device error codes.
+constexpr unsigned int kErrWaitTimeout = 1u;  // a bounded mbarrier wait gave up
+
 }  // namespace nm
 
 #define NM_CUDA_TRY(call)                                                     \
@@ -100,6 +113,77 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// ---- TMA bulk copies and mbarriers (inline PTX, sm_90+ / sm_100a) ----------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses to the same shared memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Arrive on the barrier and add `bytes` to the transaction count it waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// One-dimensional TMA bulk copy global -> shared; completion is signalled on
+// `bar` as `bytes` transaction bytes.  src, dst 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of `bar` to complete, giving up after ~2 s of
+// wall time (and after a fixed number of polls) so that no fault can turn
+// into a hang.  Returns false when it gave up.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    for (uint32_t it = 0; it < (1u << 30); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) return false;
+    }
+    return false;
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {

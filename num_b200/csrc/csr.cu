@@ -55,6 +55,9 @@ int normalise_tuning(nm_tuning& t) {
     if (t.max_rows <= 0) t.max_rows = kDefaultMaxRows;
     if (t.short_max <= 0) t.short_max = kDefaultShortMax;
     if (t.grid_mult < 0) t.grid_mult = 0;
+    if (t.stages <= 0) t.stages = kDefaultStages;
+    if (t.stages != 2 && t.stages != 3)
+        return fail(NM_ERR_INVALID, "tuning: stages must be 2 or 3 (got %d)", t.stages);
     if (t.tile != 1024 && t.tile != 2048 && t.tile != 4096)
         return fail(NM_ERR_INVALID, "tuning: tile must be 1024, 2048 or 4096 (got %d)", t.tile);
     if (t.max_rows > kThreads)
@@ -82,12 +85,17 @@ int validate_csr(const int32_t* rp, const int32_t* ci, int32_t nrows, int32_t nc
 
 int upload(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals) {
     const size_t es = dtype_size(A->dtype);
-    const int64_t nnz_pad = ((static_cast<int64_t>(A->nnz) + 3) & ~int64_t(3)) + 4;
-    NM_CUDA_TRY(cudaMalloc(&A->d_row_ptr, sizeof(int32_t) * (size_t(A->nrows) + 1)));
+    const int64_t nnz_pad = ((static_cast<int64_t>(A->nnz) + 7) & ~int64_t(7)) + 8;
+    const size_t rp_len = size_t(A->nrows) + 1 + 8;
+    NM_CUDA_TRY(cudaMalloc(&A->d_row_ptr, sizeof(int32_t) * rp_len));
     NM_CUDA_TRY(cudaMalloc(&A->d_col_idx, sizeof(int32_t) * size_t(nnz_pad)));
     NM_CUDA_TRY(cudaMalloc(&A->d_values, es * size_t(nnz_pad)));
-    NM_CUDA_TRY(cudaMemcpy(A->d_row_ptr, rp, sizeof(int32_t) * (size_t(A->nrows) + 1),
-                           cudaMemcpyHostToDevice));
+    {
+        std::vector<int32_t> rpp(rp, rp + A->nrows + 1);
+        rpp.resize(rp_len, rp[A->nrows]);
+        NM_CUDA_TRY(cudaMemcpy(A->d_row_ptr, rpp.data(), sizeof(int32_t) * rp_len,
+                               cudaMemcpyHostToDevice));
+    }
     NM_CUDA_TRY(cudaMemset(A->d_col_idx, 0, sizeof(int32_t) * size_t(nnz_pad)));
     NM_CUDA_TRY(cudaMemset(A->d_values, 0, es * size_t(nnz_pad)));
     if (A->nnz > 0) {
@@ -102,12 +110,22 @@ int rebuild_blocks(nm_csr* A) {
     std::vector<int32_t> blk;
     A->nblk = build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
                                A->tune.short_max, blk, nullptr);
+    std::vector<int4> desc(size_t(A->nblk));
+    for (int32_t b = 0; b < A->nblk; ++b)
+        desc[b] = make_int4(blk[b], blk[b + 1], A->h_row_ptr[blk[b]], A->h_row_ptr[blk[b + 1]]);
     if (A->d_blk) {
         cudaFree(A->d_blk);
         A->d_blk = nullptr;
     }
+    if (A->d_desc) {
+        cudaFree(A->d_desc);
+        A->d_desc = nullptr;
+    }
     NM_CUDA_TRY(cudaMalloc(&A->d_blk, sizeof(int32_t) * blk.size()));
+    NM_CUDA_TRY(cudaMalloc(&A->d_desc, sizeof(int4) * desc.size()));
     NM_CUDA_TRY(cudaMemcpy(A->d_blk, blk.data(), sizeof(int32_t) * blk.size(),
+                           cudaMemcpyHostToDevice));
+    NM_CUDA_TRY(cudaMemcpy(A->d_desc, desc.data(), sizeof(int4) * desc.size(),
                            cudaMemcpyHostToDevice));
     return NM_OK;
 }
@@ -130,6 +148,7 @@ int finish_create(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* v
 }  // namespace
 
 int spmv_grid(const nm_csr* A, int ctas_per_sm) {
+    // Persistent grid: every CTA that fits (or grid_mult per SM when set).
     const int mult = A->tune.grid_mult > 0 ? A->tune.grid_mult : ctas_per_sm;
     const int64_t g = int64_t(sm_count()) * mult;
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, A->nblk)));
@@ -143,6 +162,7 @@ nm_csr::~nm_csr() {
     if (d_col_idx) cudaFree(d_col_idx);
     if (d_values) cudaFree(d_values);
     if (d_blk) cudaFree(d_blk);
+    if (d_desc) cudaFree(d_desc);
 }
 
 using nm::fail;
@@ -165,7 +185,7 @@ extern "C" int nm_csr_create(const int32_t* row_ptr, const int32_t* col_idx, con
     A->ncols = ncols;
     A->nnz = row_ptr[nrows];
     A->dtype = dtype;
-    A->tune = nm_tuning{0, 0, 0, 0};
+    A->tune = nm_tuning{0, 0, 0, 0, 0};
     nm::normalise_tuning(A->tune);
     return nm::finish_create(A, row_ptr, col_idx, values, out);
 }
@@ -221,7 +241,7 @@ extern "C" int nm_csr_create_batched(int32_t count, const int32_t* nrows, const 
     A->ncols = static_cast<int32_t>(tot_cols);
     A->nnz = static_cast<int32_t>(tot_nnz);
     A->dtype = dtype;
-    A->tune = nm_tuning{0, 0, 0, 0};
+    A->tune = nm_tuning{0, 0, 0, 0, 0};
     nm::normalise_tuning(A->tune);
     A->batch_row_off = row_off;
     A->batch_col_off = col_off;
@@ -250,6 +270,11 @@ extern "C" int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t) {
     nm::clear_error();
     if (!A || !t) return fail(NM_ERR_INVALID, "nm_csr_set_tuning: NULL argument");
     nm_tuning nt = *t;
+    if (nt.tile <= 0) nt.tile = A->tune.tile;
+    if (nt.max_rows <= 0) nt.max_rows = A->tune.max_rows;
+    if (nt.short_max <= 0) nt.short_max = A->tune.short_max;
+    if (nt.grid_mult < 0) nt.grid_mult = A->tune.grid_mult;
+    if (nt.stages <= 0) nt.stages = A->tune.stages;
     int st = nm::normalise_tuning(nt);
     if (st != NM_OK) return st;
     {

@@ -1,12 +1,16 @@
 // csr.cuh -- internal layout of a device CSR matrix.
 //
 // HBM layout (one cudaMalloc each, 256-byte aligned):
-//   row_ptr  int32[nrows + 1]
-//   col_idx  int32[nnz_pad]      nnz_pad = round_up(nnz, 4) + 4, pad = column 0
-//   values   V[nnz_pad]          pad = 0
-//   blk      int32[nblk + 1]     row-block boundaries (see build_row_blocks)
-// The padding lets every thread load 4 consecutive nonzeros with one 16-byte
-// access from a 4-aligned index without reading past the allocation.
+//   row_ptr  int32[nrows + 1 + 8]  pad = nnz
+//   col_idx  int32[nnz_pad]        nnz_pad = round_up(nnz, 8) + 8, pad = column 0
+//   values   V[nnz_pad]            pad = 0
+//   blk      int32[nblk + 1]       row-block boundaries (see build_row_blocks)
+//   desc     int4[nblk]            per block {first row, end row, first nonzero,
+//                                  end nonzero}: one 16-byte load per block
+// The padding lets the TMA bulk copies of a block start and end on 16-byte
+// boundaries (nonzeros rounded to multiples of 8, row_ptr to multiples of 4),
+// and lets a thread load 4 consecutive nonzeros with one 16-byte access,
+// without leaving the allocation.
 #pragma once
 
 #include <memory>
@@ -25,7 +29,7 @@ struct CsrView {
     const int32_t* __restrict__ row_ptr;
     const int32_t* __restrict__ col_idx;
     const V* __restrict__ values;
-    const int32_t* __restrict__ blk;
+    const int4* __restrict__ desc;  // per block {r0, r1, z0, z1}
     int32_t nblk;
     int32_t nrows;
     int32_t short_max;
@@ -35,6 +39,7 @@ struct CsrView {
 constexpr int kDefaultTile = 2048;
 constexpr int kDefaultMaxRows = kThreads;
 constexpr int kDefaultShortMax = 32;
+constexpr int kDefaultStages = 2;
 
 // Row-block partition rule, shared by the device library and restated by the
 // CPU oracle (oracle.c, or_row_blocks).  Returns nblk; blk gets nblk+1 entries.
@@ -51,6 +56,7 @@ struct nm_csr {
     int32_t* d_col_idx = nullptr;
     void* d_values = nullptr;
     int32_t* d_blk = nullptr;
+    int4* d_desc = nullptr;
     int32_t nblk = 0;
     nm_tuning tune{};
     std::vector<int32_t> h_row_ptr;  // kept to rebuild the partition on retuning
@@ -63,7 +69,7 @@ struct nm_csr {
     template <typename V>
     nm::CsrView<V> view() const {
         return nm::CsrView<V>{d_row_ptr, d_col_idx, static_cast<const V*>(d_values),
-                              d_blk,     nblk,      nrows,
+                              d_desc,    nblk,      nrows,
                               tune.short_max};
     }
 };

@@ -3,28 +3,46 @@
 
 namespace nm {
 
-template <typename V, typename X, typename A, int TILE>
+template <typename V, typename X, typename A, int TILE, int STAGES>
 __global__ void __launch_bounds__(kThreads)
-    spmv_kernel(const CsrView<V> M, const X* __restrict__ x, X* __restrict__ y) {
-    __shared__ SpmvSmem<A, TILE> sm;
+    spmv_kernel(const CsrView<V> M, const X* __restrict__ x, X* __restrict__ y,
+                unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<V, A, TILE, STAGES>*>(smem_raw);
     StoreEpi<X, A> epi{y};
-    for (int32_t b = blockIdx.x; b < M.nblk; b += gridDim.x)
-        spmv_block<V, X, A, TILE>(M, M.blk[b], M.blk[b + 1], x, sm, epi);
+    spmv_pipeline<V, X, A, TILE, STAGES>(M, x, sm, epi, err);
+}
+
+template <typename V, typename X, typename A, int TILE, int STAGES>
+static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+    const CsrView<V> M = Am->view<V>();
+    constexpr size_t smem = spmv_smem_bytes<V, A, TILE, STAGES>();
+    auto* fn = spmv_kernel<V, X, A, TILE, STAGES>;
+    int occ = 0;
+    int st = prepare_kernel(reinterpret_cast<const void*>(fn), smem, &occ);
+    if (st != NM_OK) return st;
+    unsigned int* err = device_error_word();
+    if (!err) return fail(NM_ERR_CUDA, "spmv: cannot map the device error word");
+    const int grid = spmv_grid(Am, occ);
+    fn<<<grid, kThreads, smem, s>>>(M, x, y, err);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+template <typename V, typename X, typename A, int TILE>
+static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+    if (Am->tune.stages == 3) return launch_tile<V, X, A, TILE, 3>(Am, x, y, s);
+    return launch_tile<V, X, A, TILE, 2>(Am, x, y, s);
 }
 
 template <typename V, typename X, typename A>
 static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    const CsrView<V> M = Am->view<V>();
-    // One CTA per row block unless a persistent grid was requested.
-    const int grid = Am->tune.grid_mult > 0 ? spmv_grid(Am, Am->tune.grid_mult) : Am->nblk;
     switch (Am->tune.tile) {
-        case 1024: spmv_kernel<V, X, A, 1024><<<grid, kThreads, 0, s>>>(M, x, y); break;
-        case 2048: spmv_kernel<V, X, A, 2048><<<grid, kThreads, 0, s>>>(M, x, y); break;
-        case 4096: spmv_kernel<V, X, A, 4096><<<grid, kThreads, 0, s>>>(M, x, y); break;
+        case 1024: return launch_stages<V, X, A, 1024>(Am, x, y, s);
+        case 2048: return launch_stages<V, X, A, 2048>(Am, x, y, s);
+        case 4096: return launch_stages<V, X, A, 4096>(Am, x, y, s);
         default: return fail(NM_ERR_INVALID, "spmv: unsupported tile %d", Am->tune.tile);
     }
-    NM_CHECK_LAUNCH();
-    return NM_OK;
 }
 
 int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {

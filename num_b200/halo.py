@@ -226,6 +226,7 @@ def dist_spmv(A_dist, x_local, y_local) -> None:
     ops = _ops_for(A_dist)
     ops.spmv(xt, yt)
     torch.cuda.current_stream(yt.device).synchronize()
+    _lib.check(_lib.load().nm_check_device_errors(), "dist_spmv")
 
 
 def _ops_for(A_dist):

@@ -35,7 +35,7 @@ except ImportError:  # pragma: no cover
 __all__ = [
     "init", "finalize", "rank", "size", "barrier", "CrsMatrix", "DistCrsMatrix", "upload_csr",
     "upload_csr_batched", "distribute_csr", "spmv", "batch_spmv", "dist_spmv", "cg_solve",
-    "cg_solve_local", "tune", "row_blocks",
+    "cg_solve_local", "tune", "tuning", "row_blocks",
 ]
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
@@ -288,9 +288,11 @@ def spmv(A: CrsMatrix, x, y, kokkoskernels: bool = True, *, async_: bool = False
     if yt.shape[0] != A.nrows:
         raise ValueError("spmv: y length != A.nrows")
     s = stream_of(yt)
-    _lib.check(_lib.load().nm_spmv(A._h, xt.data_ptr(), yt.data_ptr(), s), "spmv")
+    lib = _lib.load()
+    _lib.check(lib.nm_spmv(A._h, xt.data_ptr(), yt.data_ptr(), s), "spmv")
     if not async_:
         torch.cuda.current_stream(yt.device).synchronize()
+        _lib.check(lib.nm_check_device_errors(), "spmv")
 
 
 def batch_spmv(A: CrsMatrix, X, Y, *, async_: bool = False) -> None:
@@ -348,17 +350,22 @@ def cg_solve(A_dist: DistCrsMatrix, b, x, tol: float = 1e-10, max_iter: int = 10
 
 # ---- additions -----------------------------------------------------------------
 
-def tune(A: CrsMatrix, tile: int = 0, max_rows: int = 0, short_max: int = 0,
-         grid_mult: int = 0) -> dict:
-    """Set the row-block partition parameters of A (0 keeps the default) and
-    return the effective ones."""
-    t = _lib.Tuning(int(tile), int(max_rows), int(short_max), int(grid_mult))
-    lib = _lib.load()
-    _lib.check(lib.nm_csr_set_tuning(A._h, C.byref(t)), "tune")
+def tuning(A: CrsMatrix) -> dict:
+    """The row-block partition parameters of A."""
     out = _lib.Tuning()
-    _lib.check(lib.nm_csr_get_tuning(A._h, C.byref(out)))
+    _lib.check(_lib.load().nm_csr_get_tuning(A._h, C.byref(out)))
     return {"tile": out.tile, "max_rows": out.max_rows, "short_max": out.short_max,
-            "grid_mult": out.grid_mult}
+            "grid_mult": out.grid_mult, "stages": out.stages}
+
+
+def tune(A: CrsMatrix, tile: int = 0, max_rows: int = 0, short_max: int = 0,
+         grid_mult: int = -1, stages: int = 0) -> dict:
+    """Set the row-block partition parameters of A (tile / max_rows /
+    short_max / stages <= 0 and grid_mult < 0 keep the current value;
+    grid_mult 0 is the automatic grid) and return the effective ones."""
+    t = _lib.Tuning(int(tile), int(max_rows), int(short_max), int(grid_mult), int(stages))
+    _lib.check(_lib.load().nm_csr_set_tuning(A._h, C.byref(t)), "tune")
+    return tuning(A)
 
 
 def row_blocks(A: CrsMatrix):

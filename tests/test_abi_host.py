@@ -41,7 +41,7 @@ def _host_blocks(nmlib, rp, tile=0, max_rows=0, short_max=0):
     blk = np.empty(n + 2, np.int32)
     bins = np.empty(max(n, 1), np.int8)
     nb = C.c_int32()
-    t = _lib.Tuning(tile, max_rows, short_max, 0)
+    t = _lib.Tuning(tile, max_rows, short_max, 0, 0)
     _lib.check(nmlib.nm_row_blocks_host(rp.ctypes.data, n, C.byref(t), blk.ctypes.data,
                                         blk.shape[0], bins.ctypes.data, C.byref(nb)))
     return blk[: nb.value + 1], bins[:n]

@@ -95,7 +95,7 @@ def test_power_law_all_bins(kspmv, oracle, tuning):
     x = np.random.default_rng(1).uniform(-1, 1, A.ncols)
     y, M = _run(kspmv, A, x, tuning=tuning)
     blk, bins = kspmv.row_blocks(M)
-    t = kspmv.tune(M)  # read back effective tuning
+    t = kspmv.tuning(M)  # effective tuning, read only
     oblk, obins = oracle.row_blocks(A.row_ptr, t["tile"], t["max_rows"], t["short_max"])
     assert np.array_equal(blk, oblk) and np.array_equal(bins, obins)  # device copy == oracle
     assert (bins == 1).any()
