@@ -166,6 +166,24 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
 int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter,
                 nm_cg_result* result, void* stream);
 
+/* CG that allocates nothing.  No counterpart in the reference.  For callers
+ * that cannot call cudaMalloc when they solve: processes whose device memory
+ * is already claimed by another allocator (a framework's caching pool, a
+ * serving engine that reserves nearly all of HBM), and latency-critical loops
+ * where cudaMalloc / cudaFree would synchronise the device.  Same algorithm,
+ * kernels and result as nm_cg_local, but every scratch vector comes from one
+ * fixed device array that is part of the library (about 6.3 MB held by every
+ * GPU that loads the library, until exit) instead of a per-matrix workspace.
+ * A is a handle made earlier with nm_csr_create; b, x as in nm_cg_local.
+ * Limit: A->nrows <= 262,144 (larger matrices: NM_ERR_INVALID).  The first
+ * call on a device looks up the array's device address and sets kernel
+ * attributes; make that first call before any stream capture.  All calls
+ * share the one array (the state is reset at the start of each call); calls
+ * that overlap on the GPU would race, so this entry point serialises its host
+ * callers and synchronises `stream` before returning. */
+int nm_cg_local_static(const nm_csr* A, const double* b, double* x, double tol,
+                       int32_t max_iter, nm_cg_result* result, void* stream);
+
 /* ---- distributed slice, halo pack / unpack -------------------------------- */
 
 /* distribute_csr (src/dist_spmv.hpp:27-100; build_ghost_map

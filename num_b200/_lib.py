@@ -56,6 +56,7 @@ _SIGNATURES = {
     "nm_fill": ([i64, dbl, vp, vp], C.c_int),
     "nm_scale": ([i64, dbl, vp, vp], C.c_int),
     "nm_cg_local": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
+    "nm_cg_local_static": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
     "nm_dist_create": ([vp, vp, vp, i32, i32, i32, i32, C.POINTER(vp)], C.c_int),
     "nm_dist_destroy": ([vp], C.c_int),
     "nm_dist_plan": ([vp, vp, vp, i32, i32, i32, i32, C.POINTER(vp)], C.c_int),

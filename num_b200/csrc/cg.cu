@@ -323,3 +323,216 @@ extern "C" int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, in
     if (!A) return nm::fail(NM_ERR_INVALID, "nm_cg_local: NULL matrix");
     return nm::cg_run(A, b, x, tol, max_iter, 0, result, static_cast<cudaStream_t>(stream));
 }
+
+// ---------------------------------------------------------------------------
+// CG that allocates nothing: nm_cg_local_static.
+//
+// Who needs it: callers that cannot call cudaMalloc when they solve -- a
+// process whose device memory is already claimed by another allocator (a
+// framework's caching pool or a serving engine that reserves nearly all of
+// HBM at start-up, where a new cudaMalloc fails or fragments the pool), and
+// latency-critical loops, where cudaMalloc / cudaFree synchronise the whole
+// device and stall every other stream.  nm_cg_local caches a workspace per
+// matrix, allocated on first use; this variant instead takes r, p, Ap, the
+// CTA partial sums, the device-resident CG state and the error word from one
+// file-scope device array that is part of the loaded library (every GPU that
+// loads the library holds it, about 6.3 MB, until the process exits).
+//
+// It runs the same kernels in the same order with the same grids as
+// nm_cg_local (launched directly instead of through cached CUDA graphs, and
+// polling the state through plain copies instead of pinned buffers), so the
+// two give the same iterates.  Limits: n <= kStaticCgMaxRows rows (larger
+// matrices are rejected with NM_ERR_INVALID); every call reuses the one
+// array, so it keeps the previous call's contents (the state, the arrival
+// counter and the error word are reset at the start of each call) and calls
+// that overlap on the GPU would race -- this entry point serialises its host
+// callers and synchronises `stream` before returning.
+// ---------------------------------------------------------------------------
+namespace nm {
+namespace {
+
+constexpr int64_t kStaticCgMaxRows = 262144;
+constexpr int kStaticCgMaxPartials = 4096;
+constexpr size_t kStaticErrOff = 512;      // error word, after the CgState
+constexpr size_t kStaticPartOff = 1024;    // CTA partial sums
+constexpr size_t kStaticVecOff = kStaticPartOff + sizeof(double) * kStaticCgMaxPartials;
+constexpr size_t kStaticVecBytes = sizeof(double) * size_t(kStaticCgMaxRows);
+constexpr size_t kStaticBytes = kStaticVecOff + 3 * kStaticVecBytes;
+static_assert(sizeof(CgState) <= kStaticErrOff, "CgState must fit its slot");
+static_assert(kStaticVecOff % 256 == 0 && kStaticVecBytes % 256 == 0, "vector alignment");
+
+// The scratch itself.  In host code this name is only a stand-in for the
+// symbol: its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_cg_static_scratch[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+struct StaticCgDevice {
+    bool ready;
+    unsigned char* base;  // device address of g_cg_static_scratch on this device
+    int sms;
+    int occ[3][2];        // CTAs per SM of cg_spmv_pap_kernel<tile, stages>
+};
+std::mutex g_static_mu;
+StaticCgDevice g_static_dev[kStaticMaxDevices];
+
+template <int TILE, int STAGES>
+int static_attr(int* occ) {
+    const void* fn = reinterpret_cast<const void*>(cg_spmv_pap_kernel<TILE, STAGES>);
+    const size_t smem = spmv_smem_bytes<double, double, TILE, STAGES>();
+    if (smem > 48 * 1024)
+        NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+    NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, kThreads, smem));
+    if (*occ < 1) return fail(NM_ERR_CUDA, "nm_cg_local_static: kernel does not fit on an SM");
+    return NM_OK;
+}
+
+// Once per device, with that device current: the scratch array's device
+// address and the kernel attributes.  Caller holds g_static_mu.
+int static_setup(int dev, StaticCgDevice** out) {
+    if (dev < 0 || dev >= kStaticMaxDevices)
+        return fail(NM_ERR_INVALID, "nm_cg_local_static: device %d not supported", dev);
+    StaticCgDevice& d = g_static_dev[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(NM_ERR_CUDA, "nm_cg_local_static: cudaGetSymbolAddress failed: %s",
+                        cudaGetErrorString(e));
+        NM_CUDA_TRY(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+        int st = NM_OK;
+        if ((st = static_attr<1024, 2>(&d.occ[0][0])) != NM_OK) return st;
+        if ((st = static_attr<1024, 3>(&d.occ[0][1])) != NM_OK) return st;
+        if ((st = static_attr<2048, 2>(&d.occ[1][0])) != NM_OK) return st;
+        if ((st = static_attr<2048, 3>(&d.occ[1][1])) != NM_OK) return st;
+        if ((st = static_attr<4096, 2>(&d.occ[2][0])) != NM_OK) return st;
+        if ((st = static_attr<4096, 3>(&d.occ[2][1])) != NM_OK) return st;
+        d.base = static_cast<unsigned char*>(p);
+        d.ready = true;
+    }
+    *out = &d;
+    return NM_OK;
+}
+
+struct StaticCgLaunch {
+    CsrView<double> M;
+    CgState* st;
+    double *r, *p, *Ap, *partials;
+    unsigned int* err;
+    int64_t n;
+    int grid_spmv, grid_vec;
+};
+
+template <int TILE, int STAGES>
+int static_spmv_pap(const StaticCgLaunch& L, const double* v, cudaStream_t s) {
+    cg_spmv_pap_kernel<TILE, STAGES>
+        <<<L.grid_spmv, kThreads, spmv_smem_bytes<double, double, TILE, STAGES>(), s>>>(
+            L.M, L.st, v, L.Ap, L.partials, L.err);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+int static_spmv_dispatch(int tile, int stages, const StaticCgLaunch& L, const double* v,
+                         cudaStream_t s) {
+    switch (tile) {
+        case 1024:
+            return stages == 3 ? static_spmv_pap<1024, 3>(L, v, s) : static_spmv_pap<1024, 2>(L, v, s);
+        case 4096:
+            return stages == 3 ? static_spmv_pap<4096, 3>(L, v, s) : static_spmv_pap<4096, 2>(L, v, s);
+        default:
+            return stages == 3 ? static_spmv_pap<2048, 3>(L, v, s) : static_spmv_pap<2048, 2>(L, v, s);
+    }
+}
+
+}  // namespace
+}  // namespace nm
+
+extern "C" int nm_cg_local_static(const nm_csr* A, const double* b, double* x, double tol,
+                                  int32_t max_iter, nm_cg_result* result, void* stream) {
+    using namespace nm;
+    clear_error();
+    if (!A || !b || !x || !result) return fail(NM_ERR_INVALID, "nm_cg_local_static: NULL argument");
+    if (A->dtype != NM_F64) return fail(NM_ERR_TYPE, "nm_cg_local_static: float64 matrices only");
+    if (A->nrows != A->ncols) return fail(NM_ERR_INVALID, "nm_cg_local_static: matrix must be square");
+    if (int64_t(A->nrows) > kStaticCgMaxRows)
+        return fail(NM_ERR_INVALID,
+                    "nm_cg_local_static: %d rows exceed the fixed scratch of %lld rows; use "
+                    "nm_cg_local",
+                    A->nrows, static_cast<long long>(kStaticCgMaxRows));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    int dev = 0;
+    NM_CUDA_TRY(cudaGetDevice(&dev));
+    StaticCgDevice* d = nullptr;
+    int st = static_setup(dev, &d);
+    if (st != NM_OK) return st;
+
+    const int ti = A->tune.tile == 1024 ? 0 : (A->tune.tile == 4096 ? 2 : 1);
+    const int si = A->tune.stages == 3 ? 1 : 0;
+    const int mult = A->tune.grid_mult > 0 ? A->tune.grid_mult : d->occ[ti][si];
+    StaticCgLaunch L;
+    L.M = A->view<double>();
+    L.n = A->nrows;
+    L.grid_spmv = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(int64_t(d->sms) * mult, A->nblk)));
+    L.grid_vec = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>((L.n + kThreads - 1) / kThreads, int64_t(d->sms) * 8)));
+    if (2 * std::max(L.grid_spmv, L.grid_vec) > kStaticCgMaxPartials)
+        return fail(NM_ERR_INVALID, "nm_cg_local_static: grid of %d CTAs exceeds the scratch",
+                    std::max(L.grid_spmv, L.grid_vec));
+    L.st = reinterpret_cast<CgState*>(d->base);
+    L.err = reinterpret_cast<unsigned int*>(d->base + kStaticErrOff);
+    L.partials = reinterpret_cast<double*>(d->base + kStaticPartOff);
+    L.r = reinterpret_cast<double*>(d->base + kStaticVecOff);
+    L.p = reinterpret_cast<double*>(d->base + kStaticVecOff + kStaticVecBytes);
+    L.Ap = reinterpret_cast<double*>(d->base + kStaticVecOff + 2 * kStaticVecBytes);
+
+    // Reset the header (state, arrival counter, error word) left by the last call.
+    unsigned char hdr[kStaticPartOff];
+    std::memset(hdr, 0, sizeof hdr);
+    CgState h;
+    std::memset(&h, 0, sizeof h);
+    h.b = b;
+    h.x = x;
+    h.tol = tol;
+    h.max_iter = max_iter;
+    h.guard = 0;
+    std::memcpy(hdr, &h, sizeof h);
+    NM_CUDA_TRY(cudaMemcpyAsync(d->base, hdr, sizeof hdr, cudaMemcpyHostToDevice, s));
+
+    // Ap = A x0 through the fused kernel (its x0.Ax0 by-product is unused;
+    // the state's alpha it leaves is overwritten before any use), then
+    // r = b - Ap, p = r, ||b||, r.r and the early exit.
+    st = static_spmv_dispatch(A->tune.tile, A->tune.stages, L, x, s);
+    if (st != NM_OK) return st;
+    cg_init_kernel<<<L.grid_vec, kThreads, 0, s>>>(L.n, L.st, L.Ap, L.r, L.p, L.partials);
+    NM_CHECK_LAUNCH();
+
+    int chunk = 8;
+    CgState o;
+    unsigned int errw = 0;
+    for (;;) {
+        NM_CUDA_TRY(cudaMemcpyAsync(hdr, d->base, sizeof hdr, cudaMemcpyDeviceToHost, s));
+        NM_CUDA_TRY(cudaStreamSynchronize(s));
+        std::memcpy(&o, hdr, sizeof o);
+        std::memcpy(&errw, hdr + kStaticErrOff, sizeof errw);
+        if (o.done || errw) break;
+        for (int i = 0; i < chunk; ++i) {
+            st = static_spmv_dispatch(A->tune.tile, A->tune.stages, L, L.p, s);
+            if (st != NM_OK) return st;
+            cg_update_xr_kernel<<<L.grid_vec, kThreads, 0, s>>>(L.n, L.st, L.p, L.Ap, L.r,
+                                                               L.partials);
+            cg_update_p_kernel<<<L.grid_vec, kThreads, 0, s>>>(L.n, L.st, L.p, L.r);
+        }
+        NM_CHECK_LAUNCH();
+        if (chunk < 64) chunk *= 2;
+    }
+    if (errw || o.status == kCgDeviceError)
+        return fail(NM_ERR_RUNTIME,
+                    "nm_cg_local_static: a device wait gave up; the solve was abandoned");
+    result->iters = o.iters;
+    result->final_res = o.final_res;
+    result->converged = o.converged;
+    return NM_OK;
+}
