@@ -51,7 +51,7 @@ typedef struct {
     int32_t max_rows;   /* max rows of a block (<= 256)                             */
     int32_t short_max;  /* rows with <= short_max nonzeros: one thread; else a warp */
     int32_t grid_mult;  /* CTAs launched per SM by the persistent SpMV grid (0: auto) */
-    int32_t stages;     /* TMA pipeline depth of the SpMV kernels: 2 or 3             */
+    int32_t stages;     /* TMA pipeline depth of the SpMV kernels: 2, 3 or 4          */
 } nm_tuning;
 
 typedef struct nm_csr nm_csr;    /* device CSR matrix (CrsMatrixHandle)   */
@@ -176,8 +176,9 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * GPU that loads the library, until exit) instead of a per-matrix workspace.
  * A is a handle made earlier with nm_csr_create; b, x as in nm_cg_local.
  * Limit: A->nrows <= 262,144 (larger matrices: NM_ERR_INVALID).  The first
- * call on a device looks up the array's device address and sets kernel
- * attributes; make that first call before any stream capture.  All calls
+ * call on a device looks up the array's device address, and the first call
+ * with each tile / stage setting sets that kernel's attributes; make those
+ * first calls before any stream capture.  All calls
  * share the one array (the state is reset at the start of each call); calls
  * that overlap on the GPU would race, so this entry point serialises its host
  * callers and synchronises `stream` before returning. */

@@ -47,7 +47,7 @@ std::mutex g_kern_mu;
 std::map<std::pair<const void*, int>, int> g_kern_occ;  // (kernel, device) -> CTAs per SM
 }  // namespace
 
-int prepare_kernel(const void* fn, size_t smem, int* ctas_per_sm) {
+int prepare_kernel(const void* fn, int threads, size_t smem, int* ctas_per_sm) {
     int dev = 0;
     NM_CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> g(g_kern_mu);
@@ -63,7 +63,7 @@ int prepare_kernel(const void* fn, size_t smem, int* ctas_per_sm) {
     NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
     int occ = 0;
-    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem));
+    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem));
     if (occ < 1) return fail(NM_ERR_CUDA, "kernel does not fit on an SM (%zu B shared)", smem);
     g_kern_occ[key] = occ;
     *ctas_per_sm = occ;

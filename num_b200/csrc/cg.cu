@@ -74,12 +74,12 @@ struct PApEpi {
 };
 
 template <int TILE, int STAGES>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kCtaThreads)
     cg_spmv_pap_kernel(const CsrView<double> M, CgState* st, const double* __restrict__ p,
                        double* __restrict__ Ap, double* partials, unsigned int* err) {
     if (__ldcg(&st->done)) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<SpmvSmem<double, double, TILE, STAGES>*>(smem_raw);
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES>*>(smem_raw);
     PApEpi epi{Ap, p, 0.0};
     const bool ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
     if (!ok && threadIdx.x == 0) {
@@ -167,11 +167,13 @@ namespace {
 template <int TILE, int STAGES>
 int prepare_cg_spmv(int* occ) {
     return prepare_kernel(reinterpret_cast<const void*>(cg_spmv_pap_kernel<TILE, STAGES>),
-                          spmv_smem_bytes<double, double, TILE, STAGES>(), occ);
+                          kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(),
+                          occ);
 }
 
 template <int TILE>
 int prepare_cg_spmv_s(int stages, int* occ) {
+    if (stages == 4) return prepare_cg_spmv<TILE, 4>(occ);
     return stages == 3 ? prepare_cg_spmv<TILE, 3>(occ) : prepare_cg_spmv<TILE, 2>(occ);
 }
 
@@ -216,9 +218,10 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
 
 template <int TILE, int STAGES>
 void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
-    const CsrView<double> M = A->view<double>();
+    CsrView<double> M = A->view<double>();
+    M.stage_x = 1;  // p is a workspace vector (256-byte aligned)
     cg_spmv_pap_kernel<TILE, STAGES>
-        <<<ws->grid_spmv, kThreads, spmv_smem_bytes<double, double, TILE, STAGES>(), s>>>(
+        <<<ws->grid_spmv, kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(), s>>>(
             M, ws->st, ws->p, ws->Ap, ws->partials, ws->err);
     cg_update_xr_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, ws->p, ws->Ap, ws->r,
                                                           ws->partials);
@@ -227,7 +230,8 @@ void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
 
 template <int TILE>
 void launch_iteration_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
-    if (A->tune.stages == 3) launch_iteration_t<TILE, 3>(A, ws, s);
+    if (A->tune.stages == 4) launch_iteration_t<TILE, 4>(A, ws, s);
+    else if (A->tune.stages == 3) launch_iteration_t<TILE, 3>(A, ws, s);
     else launch_iteration_t<TILE, 2>(A, ws, s);
 }
 
@@ -370,7 +374,7 @@ struct StaticCgDevice {
     bool ready;
     unsigned char* base;  // device address of g_cg_static_scratch on this device
     int sms;
-    int occ[3][2];        // CTAs per SM of cg_spmv_pap_kernel<tile, stages>
+    int occ[3][3];        // CTAs per SM of cg_spmv_pap_kernel<tile, stages>; 0 = not set up
 };
 std::mutex g_static_mu;
 StaticCgDevice g_static_dev[kStaticMaxDevices];
@@ -378,13 +382,13 @@ StaticCgDevice g_static_dev[kStaticMaxDevices];
 template <int TILE, int STAGES>
 int static_attr(int* occ) {
     const void* fn = reinterpret_cast<const void*>(cg_spmv_pap_kernel<TILE, STAGES>);
-    const size_t smem = spmv_smem_bytes<double, double, TILE, STAGES>();
+    const size_t smem = spmv_smem_bytes<double, double, double, TILE, STAGES>();
     if (smem > 48 * 1024)
         NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem)));
     NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
-    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, kThreads, smem));
+    NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, kCtaThreads, smem));
     if (*occ < 1) return fail(NM_ERR_CUDA, "nm_cg_local_static: kernel does not fit on an SM");
     return NM_OK;
 }
@@ -402,13 +406,6 @@ int static_setup(int dev, StaticCgDevice** out) {
             return fail(NM_ERR_CUDA, "nm_cg_local_static: cudaGetSymbolAddress failed: %s",
                         cudaGetErrorString(e));
         NM_CUDA_TRY(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
-        int st = NM_OK;
-        if ((st = static_attr<1024, 2>(&d.occ[0][0])) != NM_OK) return st;
-        if ((st = static_attr<1024, 3>(&d.occ[0][1])) != NM_OK) return st;
-        if ((st = static_attr<2048, 2>(&d.occ[1][0])) != NM_OK) return st;
-        if ((st = static_attr<2048, 3>(&d.occ[1][1])) != NM_OK) return st;
-        if ((st = static_attr<4096, 2>(&d.occ[2][0])) != NM_OK) return st;
-        if ((st = static_attr<4096, 3>(&d.occ[2][1])) != NM_OK) return st;
         d.base = static_cast<unsigned char*>(p);
         d.ready = true;
     }
@@ -427,23 +424,34 @@ struct StaticCgLaunch {
 
 template <int TILE, int STAGES>
 int static_spmv_pap(const StaticCgLaunch& L, const double* v, cudaStream_t s) {
+    CsrView<double> M = L.M;
+    M.stage_x = (reinterpret_cast<uintptr_t>(v) % 16) == 0;
     cg_spmv_pap_kernel<TILE, STAGES>
-        <<<L.grid_spmv, kThreads, spmv_smem_bytes<double, double, TILE, STAGES>(), s>>>(
-            L.M, L.st, v, L.Ap, L.partials, L.err);
+        <<<L.grid_spmv, kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(), s>>>(
+            M, L.st, v, L.Ap, L.partials, L.err);
     NM_CHECK_LAUNCH();
     return NM_OK;
+}
+
+template <int TILE>
+int static_spmv_stages(int stages, const StaticCgLaunch& L, const double* v, cudaStream_t s) {
+    if (stages == 4) return static_spmv_pap<TILE, 4>(L, v, s);
+    return stages == 3 ? static_spmv_pap<TILE, 3>(L, v, s) : static_spmv_pap<TILE, 2>(L, v, s);
 }
 
 int static_spmv_dispatch(int tile, int stages, const StaticCgLaunch& L, const double* v,
                          cudaStream_t s) {
     switch (tile) {
-        case 1024:
-            return stages == 3 ? static_spmv_pap<1024, 3>(L, v, s) : static_spmv_pap<1024, 2>(L, v, s);
-        case 4096:
-            return stages == 3 ? static_spmv_pap<4096, 3>(L, v, s) : static_spmv_pap<4096, 2>(L, v, s);
-        default:
-            return stages == 3 ? static_spmv_pap<2048, 3>(L, v, s) : static_spmv_pap<2048, 2>(L, v, s);
+        case 1024: return static_spmv_stages<1024>(stages, L, v, s);
+        case 4096: return static_spmv_stages<4096>(stages, L, v, s);
+        default: return static_spmv_stages<2048>(stages, L, v, s);
     }
+}
+
+template <int TILE>
+int static_attr_stages(int stages, int* occ) {
+    if (stages == 4) return static_attr<TILE, 4>(occ);
+    return stages == 3 ? static_attr<TILE, 3>(occ) : static_attr<TILE, 2>(occ);
 }
 
 }  // namespace
@@ -470,7 +478,18 @@ extern "C" int nm_cg_local_static(const nm_csr* A, const double* b, double* x, d
     if (st != NM_OK) return st;
 
     const int ti = A->tune.tile == 1024 ? 0 : (A->tune.tile == 4096 ? 2 : 1);
-    const int si = A->tune.stages == 3 ? 1 : 0;
+    const int si = A->tune.stages - 2;
+    if (d->occ[ti][si] == 0) {  // kernel attributes of this variant, once per device
+        switch (ti) {
+            case 0: st = static_attr_stages<1024>(A->tune.stages, &d->occ[ti][si]); break;
+            case 2: st = static_attr_stages<4096>(A->tune.stages, &d->occ[ti][si]); break;
+            default: st = static_attr_stages<2048>(A->tune.stages, &d->occ[ti][si]); break;
+        }
+        if (st != NM_OK) {
+            d->occ[ti][si] = 0;
+            return st;
+        }
+    }
     const int mult = A->tune.grid_mult > 0 ? A->tune.grid_mult : d->occ[ti][si];
     StaticCgLaunch L;
     L.M = A->view<double>();

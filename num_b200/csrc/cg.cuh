@@ -49,7 +49,8 @@ struct CgWorkspace {
 // Grid of the grid-stride vector kernels for n elements.
 int vec_grid(int64_t n);
 
-// Last-CTA grid reduction: every CTA passes K partial sums (valid in thread 0);
+// Last-CTA grid reduction: every CTA passes K partial sums (valid in thread 0;
+// `red` has one entry per warp of the CTA);
 // returns true on thread 0 of the CTA that arrives last, with the grid totals
 // summed in a fixed order (so results are bit-reproducible for a fixed grid).
 // The counter is reset for the next launch.  Call from all threads.
@@ -71,7 +72,7 @@ __device__ __forceinline__ bool grid_reduce_last(const double (&part)[K], double
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         double s = 0.0;
-        for (unsigned i = threadIdx.x; i < gridDim.x; i += kThreads)
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
             s += __ldcg(partials + size_t(k) * gridDim.x + i);
         tot[k] = block_sum(s, red);
     }

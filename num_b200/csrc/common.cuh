@@ -31,8 +31,8 @@ unsigned int* device_error_word();
 
 // Opts kernel `fn` into `smem` bytes of dynamic shared memory and the
 // maximum shared-memory carveout on the current device (once per device) and
-// returns how many CTAs of kThreads threads fit on one SM.
-int prepare_kernel(const void* fn, size_t smem, int* ctas_per_sm);
+// returns how many CTAs of `threads` threads fit on one SM.
+int prepare_kernel(const void* fn, int threads, size_t smem, int* ctas_per_sm);
 
 // Device error codes.
 constexpr unsigned int kErrWaitTimeout = 1u;  // a bounded mbarrier wait gave up
@@ -192,9 +192,10 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-// Deterministic CTA-wide sum: fixed shuffle tree per warp, then warp 0 adds the
-// warp totals in warp order.  Result is valid in thread 0 only.  `scratch`
-// needs kWarps entries.  Contains __syncthreads(); call from all threads.
+// Deterministic CTA-wide sum: fixed shuffle tree per warp, then thread 0 adds
+// the warp totals in warp order.  Result is valid in thread 0 only.
+// `scratch` needs one entry per warp of the CTA.  Contains __syncthreads();
+// call from all threads.
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* scratch) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -203,8 +204,8 @@ __device__ __forceinline__ T block_sum(T v, T* scratch) {
     __syncthreads();
     T s = T(0);
     if (threadIdx.x == 0) {
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) s += scratch[w];
+        const int nw = static_cast<int>(blockDim.x) >> 5;
+        for (int w = 0; w < nw; ++w) s += scratch[w];
     }
     __syncthreads();
     return s;

@@ -4,8 +4,10 @@
 // rows-per-team pick of the reference custom kernel (src/spmv_kernel.hpp:102-109)
 // with a per-row-block partition computed once at upload.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <string>
+#include <thread>
 
 #include "cg.cuh"
 #include "csr.cuh"
@@ -39,6 +41,45 @@ int build_row_blocks(const int32_t* rp, int32_t nrows, int tile, int max_rows, i
     return static_cast<int>(blk.size()) - 1;
 }
 
+void block_xwindows(const int32_t* ci, int32_t z0, int32_t z1, int32_t ncols, int xw,
+                    std::vector<int32_t>& c, int4* xs, int4* xl) {
+    *xs = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
+    *xl = make_int4(0, 0, 0, 0);
+    if (z1 <= z0) return;
+    c.assign(ci + z0, ci + z1);
+    std::sort(c.begin(), c.end());
+    int32_t st[kXSeg], en[kXSeg];
+    int nseg = 0;
+    int32_t cs = c[0] & ~3, ce = (c[0] | 3) + 1;
+    for (size_t k = 1; k < c.size(); ++k) {
+        const int32_t a = c[k] & ~3, e = (c[k] | 3) + 1;
+        if (a <= ce + kXGap) {
+            ce = std::max(ce, e);
+        } else {
+            if (nseg == kXSeg) return;  // too many windows: gather from global
+            st[nseg] = cs;
+            en[nseg] = ce;
+            ++nseg;
+            cs = a;
+            ce = e;
+        }
+    }
+    if (nseg == kXSeg) return;
+    st[nseg] = cs;
+    en[nseg] = ce;
+    ++nseg;
+    int64_t total = 0;
+    for (int k = 0; k < nseg; ++k) total += en[k] - st[k];
+    if (total > xw || en[nseg - 1] > (ncols & ~3)) return;  // too wide, or would read past x
+    int32_t sv[kXSeg] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX}, lv[kXSeg] = {0, 0, 0, 0};
+    for (int k = 0; k < nseg; ++k) {
+        sv[k] = st[k];
+        lv[k] = en[k] - st[k];
+    }
+    *xs = make_int4(sv[0], sv[1], sv[2], sv[3]);
+    *xl = make_int4(lv[0], lv[1], lv[2], lv[3]);
+}
+
 namespace {
 
 size_t dtype_size(int dtype) {
@@ -56,8 +97,8 @@ int normalise_tuning(nm_tuning& t) {
     if (t.short_max <= 0) t.short_max = kDefaultShortMax;
     if (t.grid_mult < 0) t.grid_mult = 0;
     if (t.stages <= 0) t.stages = kDefaultStages;
-    if (t.stages != 2 && t.stages != 3)
-        return fail(NM_ERR_INVALID, "tuning: stages must be 2 or 3 (got %d)", t.stages);
+    if (t.stages < 2 || t.stages > 4)
+        return fail(NM_ERR_INVALID, "tuning: stages must be 2, 3 or 4 (got %d)", t.stages);
     if (t.tile != 1024 && t.tile != 2048 && t.tile != 4096)
         return fail(NM_ERR_INVALID, "tuning: tile must be 1024, 2048 or 4096 (got %d)", t.tile);
     if (t.max_rows > kThreads)
@@ -110,9 +151,39 @@ int rebuild_blocks(nm_csr* A) {
     std::vector<int32_t> blk;
     A->nblk = build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
                                A->tune.short_max, blk, nullptr);
-    std::vector<int4> desc(size_t(A->nblk));
-    for (int32_t b = 0; b < A->nblk; ++b)
-        desc[b] = make_int4(blk[b], blk[b + 1], A->h_row_ptr[blk[b]], A->h_row_ptr[blk[b + 1]]);
+    std::vector<BlockDesc> desc(size_t(A->nblk));
+    const int32_t* rp = A->h_row_ptr.data();
+    const int32_t* ci = A->h_col_idx.data();
+    const int tile = A->tune.tile;
+    const int short_max = A->tune.short_max;
+    const int32_t nb = A->nblk, ncols = A->ncols;
+    auto fill = [&](int32_t b0, int32_t b1) {
+        std::vector<int32_t> scratch;
+        for (int32_t b = b0; b < b1; ++b) {
+            BlockDesc& d = desc[b];
+            const int32_t z0 = rp[blk[b]], z1 = rp[blk[b + 1]];
+            d.rz = make_int4(blk[b], blk[b + 1], z0, z1);
+            int32_t nlong = 0;
+            for (int32_t r = blk[b]; r < blk[b + 1]; ++r) nlong += (rp[r + 1] - rp[r]) > short_max;
+            d.aux = make_int4(nlong, 0, 0, 0);
+            if (z1 - z0 > tile) {
+                d.xs = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
+                d.xl = make_int4(0, 0, 0, 0);
+            } else {
+                block_xwindows(ci, z0, z1, ncols, tile, scratch, &d.xs, &d.xl);
+            }
+        }
+    };
+    const int nthr = static_cast<int>(std::min<int64_t>(
+        std::max(1u, std::thread::hardware_concurrency()), std::max<int64_t>(1, nb / 256)));
+    if (nthr <= 1) {
+        fill(0, nb);
+    } else {
+        std::vector<std::thread> th;
+        for (int i = 0; i < nthr; ++i)
+            th.emplace_back(fill, int32_t(int64_t(nb) * i / nthr), int32_t(int64_t(nb) * (i + 1) / nthr));
+        for (auto& t : th) t.join();
+    }
     if (A->d_blk) {
         cudaFree(A->d_blk);
         A->d_blk = nullptr;
@@ -122,10 +193,10 @@ int rebuild_blocks(nm_csr* A) {
         A->d_desc = nullptr;
     }
     NM_CUDA_TRY(cudaMalloc(&A->d_blk, sizeof(int32_t) * blk.size()));
-    NM_CUDA_TRY(cudaMalloc(&A->d_desc, sizeof(int4) * desc.size()));
+    NM_CUDA_TRY(cudaMalloc(&A->d_desc, sizeof(BlockDesc) * desc.size()));
     NM_CUDA_TRY(cudaMemcpy(A->d_blk, blk.data(), sizeof(int32_t) * blk.size(),
                            cudaMemcpyHostToDevice));
-    NM_CUDA_TRY(cudaMemcpy(A->d_desc, desc.data(), sizeof(int4) * desc.size(),
+    NM_CUDA_TRY(cudaMemcpy(A->d_desc, desc.data(), sizeof(BlockDesc) * desc.size(),
                            cudaMemcpyHostToDevice));
     return NM_OK;
 }
@@ -135,6 +206,7 @@ int finish_create(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* v
     int st = upload(A, rp, ci, vals);
     if (st == NM_OK) {
         A->h_row_ptr.assign(rp, rp + A->nrows + 1);
+        A->h_col_idx.assign(ci, ci + A->nnz);
         st = rebuild_blocks(A);
     }
     if (st != NM_OK) {

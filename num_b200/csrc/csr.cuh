@@ -5,8 +5,7 @@
 //   col_idx  int32[nnz_pad]        nnz_pad = round_up(nnz, 8) + 8, pad = column 0
 //   values   V[nnz_pad]            pad = 0
 //   blk      int32[nblk + 1]       row-block boundaries (see build_row_blocks)
-//   desc     int4[nblk]            per block {first row, end row, first nonzero,
-//                                  end nonzero}: one 16-byte load per block
+//   desc     BlockDesc[nblk]       per block rows, nonzeros and x windows
 // The padding lets the TMA bulk copies of a block start and end on 16-byte
 // boundaries (nonzeros rounded to multiples of 8, row_ptr to multiples of 4),
 // and lets a thread load 4 consecutive nonzeros with one 16-byte access,
@@ -23,16 +22,33 @@ namespace nm {
 
 struct CgWorkspace;  // cg.cu
 
+// Row-block descriptor, one 64-byte record per block.
+//   rz = {first row, end row, first nonzero, end nonzero}
+//   xs = starts of the block's x windows (xs.x < 0: no windows; unused: INT_MAX)
+//   xl = lengths of the x windows (0: unused)
+// The x windows are up to kXSeg ranges of x, each starting and ending on a
+// multiple of 4 elements, that together hold every column the block's
+// nonzeros reference; the SpMV kernels stage them with the block's nonzeros.
+constexpr int kXSeg = 4;
+constexpr int kXGap = 16;  // gaps up to this many elements are bridged
+struct BlockDesc {
+    int4 rz;
+    int4 xs;
+    int4 xl;
+    int4 aux;  // {rows reduced by a warp (nnz > short_max), 0, 0, 0}
+};
+
 // Kernel-side view of a matrix.
 template <typename V>
 struct CsrView {
     const int32_t* __restrict__ row_ptr;
     const int32_t* __restrict__ col_idx;
     const V* __restrict__ values;
-    const int4* __restrict__ desc;  // per block {r0, r1, z0, z1}
+    const BlockDesc* __restrict__ desc;
     int32_t nblk;
     int32_t nrows;
     int32_t short_max;
+    int32_t stage_x;  // 1: x windows are staged (x 16-byte aligned); 0: gather from global
 };
 
 // Default row-block parameters.
@@ -40,6 +56,11 @@ constexpr int kDefaultTile = 2048;
 constexpr int kDefaultMaxRows = kThreads;
 constexpr int kDefaultShortMax = 32;
 constexpr int kDefaultStages = 2;
+
+// x windows of the multi-row block with nonzeros [z0, z1) (see BlockDesc);
+// xw = largest total window length, ncols = length of x.
+void block_xwindows(const int32_t* col_idx, int32_t z0, int32_t z1, int32_t ncols, int xw,
+                    std::vector<int32_t>& scratch, int4* xs, int4* xl);
 
 // Row-block partition rule, shared by the device library and restated by the
 // CPU oracle (oracle.c, or_row_blocks).  Returns nblk; blk gets nblk+1 entries.
@@ -56,10 +77,11 @@ struct nm_csr {
     int32_t* d_col_idx = nullptr;
     void* d_values = nullptr;
     int32_t* d_blk = nullptr;
-    int4* d_desc = nullptr;
+    nm::BlockDesc* d_desc = nullptr;
     int32_t nblk = 0;
     nm_tuning tune{};
     std::vector<int32_t> h_row_ptr;  // kept to rebuild the partition on retuning
+    std::vector<int32_t> h_col_idx;  // kept to rebuild the x windows on retuning
     // Many-matrix handles: per-matrix row / column offsets (count + 1 each).
     std::vector<int32_t> batch_row_off, batch_col_off;
     std::mutex cg_mutex;
@@ -70,7 +92,7 @@ struct nm_csr {
     nm::CsrView<V> view() const {
         return nm::CsrView<V>{d_row_ptr, d_col_idx, static_cast<const V*>(d_values),
                               d_desc,    nblk,      nrows,
-                              tune.short_max};
+                              tune.short_max, 0};
     }
 };
 

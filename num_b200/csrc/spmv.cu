@@ -4,33 +4,35 @@
 namespace nm {
 
 template <typename V, typename X, typename A, int TILE, int STAGES>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kCtaThreads)
     spmv_kernel(const CsrView<V> M, const X* __restrict__ x, X* __restrict__ y,
                 unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<SpmvSmem<V, A, TILE, STAGES>*>(smem_raw);
+    auto& sm = *reinterpret_cast<SpmvSmem<V, X, A, TILE, STAGES>*>(smem_raw);
     StoreEpi<X, A> epi{y};
     spmv_pipeline<V, X, A, TILE, STAGES>(M, x, sm, epi, err);
 }
 
 template <typename V, typename X, typename A, int TILE, int STAGES>
 static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    const CsrView<V> M = Am->view<V>();
-    constexpr size_t smem = spmv_smem_bytes<V, A, TILE, STAGES>();
+    CsrView<V> M = Am->view<V>();
+    M.stage_x = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+    constexpr size_t smem = spmv_smem_bytes<V, X, A, TILE, STAGES>();
     auto* fn = spmv_kernel<V, X, A, TILE, STAGES>;
     int occ = 0;
-    int st = prepare_kernel(reinterpret_cast<const void*>(fn), smem, &occ);
+    int st = prepare_kernel(reinterpret_cast<const void*>(fn), kCtaThreads, smem, &occ);
     if (st != NM_OK) return st;
     unsigned int* err = device_error_word();
     if (!err) return fail(NM_ERR_CUDA, "spmv: cannot map the device error word");
     const int grid = spmv_grid(Am, occ);
-    fn<<<grid, kThreads, smem, s>>>(M, x, y, err);
+    fn<<<grid, kCtaThreads, smem, s>>>(M, x, y, err);
     NM_CHECK_LAUNCH();
     return NM_OK;
 }
 
 template <typename V, typename X, typename A, int TILE>
 static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+    if (Am->tune.stages == 4) return launch_tile<V, X, A, TILE, 4>(Am, x, y, s);
     if (Am->tune.stages == 3) return launch_tile<V, X, A, TILE, 3>(Am, x, y, s);
     return launch_tile<V, X, A, TILE, 2>(Am, x, y, s);
 }

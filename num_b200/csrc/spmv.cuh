@@ -1,96 +1,178 @@
 // spmv.cuh -- device body of the row-block CSR SpMV, shared by the plain SpMV
 // kernel and the fused CG kernel.
 //
-// Persistent CTAs (256 threads) walk the row blocks b = blockIdx.x + k*gridDim.x.
-// Each block's col_idx, values and row_ptr slices are brought into shared
-// memory by TMA bulk copies (cp.async.bulk, one elected thread), completion
-// tracked by an mbarrier per stage; STAGES stages form a ring, so the copies
-// of the next blocks are in flight while the current one is reduced:
+// Persistent, warp-specialised CTAs of 288 threads walk the row blocks
+// b = blockIdx.x + k*gridDim.x:
 //
-//  * multi-row block (nnz <= TILE): every thread multiplies staged values
-//    with x[col] (gathered through the read-only path; x stays in L2) and
-//    writes the product back over its staged operand.  Rows with
-//    <= short_max nonzeros are then summed by one thread each, serially in
-//    CSR order (bit-identical to the reference's serial row loop,
-//    src/spmv_kernel.hpp:90-97); longer rows by one warp each.
-//  * single-row block (nnz > TILE): nothing is staged; the whole CTA strides
-//    the row with 16-byte loads and reduces with a deterministic CTA-wide sum.
+//  * one producer warp (warp 8, one lane) brings each block's col_idx,
+//    values, row_ptr slice and x windows into a ring of STAGES shared-memory
+//    stages with TMA bulk copies (cp.async.bulk); a `full` mbarrier per stage
+//    counts the transaction bytes, an `empty` mbarrier per stage counts the
+//    consumer warps that have released it, so the producer runs up to STAGES
+//    blocks ahead of the consumers;
+//  * eight consumer warps (256 threads, named barrier 1) compute the block:
+//    every thread multiplies staged values with the staged x window entries
+//    (x[col] from global memory when the block has no windows), writes the
+//    products back over the staged operands, and rows with <= short_max
+//    nonzeros are summed by one thread each, serially in CSR order
+//    (bit-identical to the reference's serial row loop,
+//    src/spmv_kernel.hpp:90-97); longer rows by one warp each.  A block that
+//    is one row with more than TILE nonzeros is read straight from global
+//    memory by all consumers and reduced with a deterministic sum.
+//
+// A block without warp rows costs the consumers one named barrier.
 //
 // The epilogue functor receives (row, value) exactly once per row, on one
-// thread; CG uses it to store Ap and to accumulate p.Ap on the fly.
+// consumer thread; CG uses it to store Ap and to accumulate p.Ap on the fly.
 //
 // Alignment (TMA bulk copies need 16-byte aligned addresses and sizes): the
-// staged nonzero range is [z0 & ~7, (z1 + 7) & ~7) and the row_ptr range
-// [r0 & ~3, (r1 + 4) & ~3); the device arrays are padded so these never leave
-// the allocation (see upload in csr.cu).
+// staged nonzero range is [z0 & ~7, (z1 + 7) & ~7), the row_ptr range
+// [r0 & ~3, (r1 + 4) & ~3), x windows start and end on multiples of 4 elements
+// inside [0, ncols & ~3); the device arrays are padded so these never leave
+// the allocation (see upload in csr.cu), and windows are used only when x is
+// 16-byte aligned.
+//
+// Every mbarrier wait is bounded (mbar_wait_bounded).  When one gives up the
+// kernel sets the device error word, the consumers stop, and the producer
+// waits (bounded again) for its copies still in flight before the CTA exits.
 #pragma once
 
 #include "csr.cuh"
 
 namespace nm {
 
-template <typename V, int TILE>
+constexpr int kConsumers = kThreads;        // 8 consumer warps
+constexpr int kCtaThreads = kThreads + 32;  // + 1 producer warp
+constexpr int kProducerWarp = kWarps;
+
+// Barrier among the 256 consumer threads only (id 1; id 0 is __syncthreads).
+__device__ __forceinline__ void consumer_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory");
+}
+
+__device__ __forceinline__ bool consumer_sync_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred q, o;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred o, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, o;\n\t}"
+        : "=r"(r)
+        : "r"(static_cast<uint32_t>(pred)), "n"(kConsumers)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Deterministic sum over the consumer threads; valid in consumer thread 0.
+template <typename T>
+__device__ __forceinline__ T consumer_sum(T v, T* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) scratch[warp] = v;
+    consumer_sync();
+    T s = T(0);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += scratch[w];
+    }
+    consumer_sync();
+    return s;
+}
+
+template <typename V, typename X, int TILE>
 struct alignas(16) SpmvStage {
     int32_t col[TILE + 16];
     V val[TILE + 16];
     int32_t rp[kThreads + 8];
+    X xw[TILE];  // the block's x windows, back to back
 };
 
-template <typename V, typename A, int TILE, int STAGES>
+template <typename V, typename X, typename A, int TILE, int STAGES>
 struct SpmvSmem {
-    SpmvStage<V, TILE> st[STAGES];
-    uint64_t bar[STAGES];
-    int32_t meta[STAGES][4];  // r0, r1, z0, z1 of the block in each stage
+    SpmvStage<V, X, TILE> st[STAGES];
+    uint64_t full[STAGES];
+    uint64_t empty[STAGES];
+    BlockDesc meta[STAGES];  // descriptor of the block in each stage
     int32_t long_rows[kThreads];
     int32_t warp_cnt[kWarps];
-    A red[kWarps];
+    A red[kWarps + 1];
 };
 
 // Product storage: over the staged values when they are as wide as the
 // accumulator, else over the staged column indices (bf16 values, float
 // products).  Each slot is read by the thread that then overwrites it.
-template <typename V, typename A, int TILE>
-__device__ __forceinline__ A* prod_slots(SpmvStage<V, TILE>& st) {
+template <typename V, typename X, typename A, int TILE>
+__device__ __forceinline__ A* prod_slots(SpmvStage<V, X, TILE>& st) {
     static_assert(sizeof(A) == sizeof(V) || sizeof(A) == sizeof(int32_t), "product slot");
     if constexpr (sizeof(A) == sizeof(V)) return reinterpret_cast<A*>(st.val);
     else return reinterpret_cast<A*>(st.col);
 }
 
-// Issued by one thread: stage the block described by d into stage s.
-template <typename V, typename A, int TILE, int STAGES>
-__device__ __forceinline__ void spmv_issue(const CsrView<V>& M, int4 d,
-                                           SpmvSmem<V, A, TILE, STAGES>& sm, int s) {
-    const int32_t r0 = d.x, r1 = d.y, z0 = d.z, z1 = d.w;
-    sm.meta[s][0] = r0;
-    sm.meta[s][1] = r1;
-    sm.meta[s][2] = z0;
-    sm.meta[s][3] = z1;
-    if (z1 - z0 > TILE) {  // long row: read from global by the consumer
-        mbar_arrive_expect_tx(&sm.bar[s], 0u);
+__device__ __forceinline__ BlockDesc load_desc(const BlockDesc* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    BlockDesc d;
+    d.rz = __ldg(q);
+    d.xs = __ldg(q + 1);
+    d.xl = __ldg(q + 2);
+    d.aux = __ldg(q + 3);
+    return d;
+}
+
+// Producer: stage the block described by d into stage s (its nonzeros,
+// row_ptr slice and, when M.stage_x, its x windows).
+template <typename V, typename X, typename A, int TILE, int STAGES>
+__device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restrict__ x,
+                                           BlockDesc d, SpmvSmem<V, X, A, TILE, STAGES>& sm,
+                                           int s) {
+    const int32_t r0 = d.rz.x, r1 = d.rz.y, z0 = d.rz.z, z1 = d.rz.w;
+    const bool long_row = z1 - z0 > TILE;
+    const bool stage_x = !long_row && M.stage_x && d.xs.x >= 0;
+    if (!stage_x) d.xs.x = -1;
+    sm.meta[s] = d;
+    if (long_row) {  // read from global by the consumers
+        mbar_arrive_expect_tx(&sm.full[s], 0u);
         return;
     }
     const int32_t a0 = z0 & ~7, a1 = (z1 + 7) & ~7;
     const int32_t ra0 = r0 & ~3, ra1 = (r1 + 4) & ~3;
     const uint32_t ncol = static_cast<uint32_t>(a1 - a0);
     const uint32_t nrp = static_cast<uint32_t>(ra1 - ra0);
-    const uint32_t bytes = ncol * uint32_t(sizeof(int32_t) + sizeof(V)) + nrp * 4u;
-    SpmvStage<V, TILE>& st = sm.st[s];
-    mbar_arrive_expect_tx(&sm.bar[s], bytes);
+    const uint32_t nxw = stage_x ? static_cast<uint32_t>(d.xl.x + d.xl.y + d.xl.z + d.xl.w) : 0u;
+    const uint32_t bytes =
+        ncol * uint32_t(sizeof(int32_t) + sizeof(V)) + nrp * 4u + nxw * uint32_t(sizeof(X));
+    SpmvStage<V, X, TILE>& st = sm.st[s];
+    mbar_arrive_expect_tx(&sm.full[s], bytes);
     if (ncol) {
-        bulk_g2s(st.col, M.col_idx + a0, ncol * 4u, &sm.bar[s]);
-        bulk_g2s(st.val, M.values + a0, ncol * uint32_t(sizeof(V)), &sm.bar[s]);
+        bulk_g2s(st.col, M.col_idx + a0, ncol * 4u, &sm.full[s]);
+        bulk_g2s(st.val, M.values + a0, ncol * uint32_t(sizeof(V)), &sm.full[s]);
     }
-    bulk_g2s(st.rp, M.row_ptr + ra0, nrp * 4u, &sm.bar[s]);
+    bulk_g2s(st.rp, M.row_ptr + ra0, nrp * 4u, &sm.full[s]);
+    if (stage_x) {
+        const int32_t ws[kXSeg] = {d.xs.x, d.xs.y, d.xs.z, d.xs.w};
+        const int32_t wl[kXSeg] = {d.xl.x, d.xl.y, d.xl.z, d.xl.w};
+        int32_t off = 0;
+#pragma unroll
+        for (int k = 0; k < kXSeg; ++k) {
+            if (wl[k] > 0)
+                bulk_g2s(st.xw + off, x + ws[k], uint32_t(wl[k]) * uint32_t(sizeof(X)),
+                         &sm.full[s]);
+            off += wl[k];
+        }
+    }
 }
 
-// One long row (nnz > TILE) straight from global memory, whole CTA.
+// One long row (nnz > TILE) straight from global memory, all consumers.
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
 __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, int32_t r0, int32_t z0,
                                               int32_t z1, const X* __restrict__ x,
-                                              SpmvSmem<V, A, TILE, STAGES>& sm, Epi& epi) {
+                                              SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
     const int t = threadIdx.x;
     A s = A(0);
-    for (int32_t j = (z0 & ~3) + 4 * t; j < z1; j += 4 * kThreads) {
+    for (int32_t j = (z0 & ~3) + 4 * t; j < z1; j += 4 * kConsumers) {
         const int4 c = ld_stream(reinterpret_cast<const int4*>(M.col_idx + j));
         A v[4];
         Load4<V, A>::run(M.values, j, v);
@@ -101,50 +183,72 @@ __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, int32_t r0, i
             if (jj >= z0 && jj < z1) s += v[q] * static_cast<A>(__ldg(x + cc[q]));
         }
     }
-    s = block_sum(s, sm.red);
+    s = consumer_sum(s, sm.red);
     if (t == 0) epi(r0, s);
 }
 
-// A staged multi-row block.
+// Consumers: one staged multi-row block.  `ok` = this thread saw the stage
+// complete.  Returns false (uniformly) if any consumer did not.
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
-__device__ __forceinline__ void spmv_tile(const CsrView<V>& M, int s, const X* __restrict__ x,
-                                          SpmvSmem<V, A, TILE, STAGES>& sm, Epi& epi) {
+__device__ __forceinline__ bool spmv_tile(const CsrView<V>& M, int s, bool ok,
+                                          const X* __restrict__ x,
+                                          SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
-    SpmvStage<V, TILE>& st = sm.st[s];
-    const int32_t r0 = sm.meta[s][0], r1 = sm.meta[s][1];
-    const int32_t z0 = sm.meta[s][2], z1 = sm.meta[s][3];
-    const int nr = r1 - r0;
-    const int32_t a0 = z0 & ~7;
-    const int32_t roff = r0 - (r0 & ~3);  // row r0's slot in the staged row_ptr
-    const int cnt = z1 - a0;
-    A* prod = prod_slots<V, A, TILE>(st);
-
-    // products: every gather of this thread is issued before any is used
-    // (one L2 round trip per block)
-    constexpr int kPer = (TILE + 16 + kThreads - 1) / kThreads;
-    {
+    SpmvStage<V, X, TILE>& st = sm.st[s];
+    A* prod = prod_slots<V, X, A, TILE>(st);
+    if (ok) {
+        const BlockDesc d = sm.meta[s];
+        const int32_t z0 = d.rz.z, z1 = d.rz.w;
+        const int32_t a0 = z0 & ~7;
+        const int cnt = z1 - a0;
+        // column -> staged x slot: window k holds columns [xs_k, xs_k + xl_k)
+        const bool staged = d.xs.x >= 0;
+        const int32_t dl0 = -d.xs.x, dl1 = d.xl.x - d.xs.y, dl2 = d.xl.x + d.xl.y - d.xs.z,
+                      dl3 = d.xl.x + d.xl.y + d.xl.z - d.xs.w;
+        // every x read of this thread is issued before any product is formed
+        constexpr int kPer = (TILE + 16 + kConsumers - 1) / kConsumers;
         const int e0 = (z0 - a0) + t;
         int c[kPer];
         A v[kPer];
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
-            const int e = e0 + q * kThreads;
+            const int e = e0 + q * kConsumers;
             c[q] = e < cnt ? st.col[e] : -1;
             v[q] = e < cnt ? widen<V, A>(st.val[e]) : A(0);
         }
         A xv[kPer];
+        if (staged) {
 #pragma unroll
-        for (int q = 0; q < kPer; ++q) xv[q] = c[q] >= 0 ? static_cast<A>(__ldg(x + c[q])) : A(0);
+            for (int q = 0; q < kPer; ++q) {
+                const int32_t cq = c[q];
+                const int32_t dl =
+                    cq >= d.xs.w ? dl3 : (cq >= d.xs.z ? dl2 : (cq >= d.xs.y ? dl1 : dl0));
+                xv[q] = cq >= 0 ? static_cast<A>(st.xw[cq + dl]) : A(0);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kPer; ++q)
+                xv[q] = c[q] >= 0 ? static_cast<A>(__ldg(x + c[q])) : A(0);
+        }
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
-            const int e = e0 + q * kThreads;
+            const int e = e0 + q * kConsumers;
             if (e < cnt) prod[e] = mul_rn(v[q], xv[q]);
         }
+        // products overwrite staged operands that the next TMA copy into this
+        // stage will overwrite again: order them before that copy
+        fence_proxy_async_smem();
     }
-    __syncthreads();
+    if (consumer_sync_or(!ok)) return false;  // products visible; all saw the stage
 
-    // thread-per-row reduction; flag the long rows
+    const BlockDesc d = sm.meta[s];
+    const int32_t r0 = d.rz.x, r1 = d.rz.y, z0 = d.rz.z;
+    const int nr = r1 - r0;
+    const int32_t a0 = z0 & ~7;
+    const int32_t roff = r0 - (r0 & ~3);  // row r0's slot in the staged row_ptr
+
+    // thread-per-row reduction
     bool is_long = false;
     if (t < nr) {
         const int32_t s0 = st.rp[roff + t] - a0, s1 = st.rp[roff + t + 1] - a0;
@@ -162,14 +266,12 @@ __device__ __forceinline__ void spmv_tile(const CsrView<V>& M, int s, const X* _
             is_long = true;
         }
     }
-    // Returns with the stage free when no row needs a warp (the common case
-    // for stencils: one barrier).
-    if (!__syncthreads_or(is_long)) return;
+    if (d.aux.x == 0) return true;  // no warp rows in this block
 
     // deterministic list of long rows in row order (ballot + warp prefix)
     const unsigned m = __ballot_sync(0xffffffffu, is_long);
     if (lane == 0) sm.warp_cnt[warp] = __popc(m);
-    __syncthreads();
+    consumer_sync();
     int base = 0, nl = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
@@ -178,7 +280,7 @@ __device__ __forceinline__ void spmv_tile(const CsrView<V>& M, int s, const X* _
         nl += cw;
     }
     if (is_long) sm.long_rows[base + __popc(m & ((1u << lane) - 1u))] = t;
-    __syncthreads();
+    consumer_sync();
 
     // warp-per-row reduction of the long rows
     for (int q = warp; q < nl; q += kWarps) {
@@ -189,68 +291,82 @@ __device__ __forceinline__ void spmv_tile(const CsrView<V>& M, int s, const X* _
         acc = warp_sum(acc);
         if (lane == 0) epi(r0 + tt, acc);
     }
-    __syncthreads();
+    return true;
 }
 
-// The persistent pipelined loop over this CTA's row blocks.  Returns false if
-// a bounded wait gave up (the error word is set; the caller must not use its
-// partial results).  Call from all threads.
+// The persistent pipelined loop over this CTA's row blocks, for all 288
+// threads.  Returns false on the threads of a CTA where a bounded wait gave
+// up (the error word is set; partial results must not be used).  On return
+// no TMA copy into this CTA's shared memory is pending.
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
 __device__ __forceinline__ bool spmv_pipeline(const CsrView<V>& M, const X* __restrict__ x,
-                                              SpmvSmem<V, A, TILE, STAGES>& sm, Epi& epi,
+                                              SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi,
                                               unsigned int* err) {
     const int t = threadIdx.x;
-    if (t == 0) {
-#pragma unroll
-        for (int s = 0; s < STAGES; ++s) mbar_init(&sm.bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    // Thread 0 issues; it holds the descriptor of the next block to issue in
-    // registers, loaded one block ahead so its latency is off the critical path.
-    int4 next_desc = make_int4(0, 0, 0, 0);
+    const int warp = t >> 5, lane = t & 31;
     if (t == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
-            const int64_t b = int64_t(blockIdx.x) + int64_t(s) * gridDim.x;
-            if (b < M.nblk) spmv_issue<V, A, TILE, STAGES>(M, __ldg(M.desc + b), sm, s);
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], kWarps);
         }
-        const int64_t nb = int64_t(blockIdx.x) + int64_t(STAGES) * gridDim.x;
-        if (nb < M.nblk) next_desc = __ldg(M.desc + nb);
+        fence_mbar_init();
     }
-    uint32_t parity = 0;  // bit s: phase parity to wait for on stage s
+    __syncthreads();
+
+    if (warp == kProducerWarp) {
+        if (lane != 0) return true;
+        // ---- producer ----
+        uint32_t full_par = 0, empty_par = 0;  // bit s: parity of the next phase
+        uint32_t used = 0;                     // bit s: stage s has been issued into
+        bool ok = true;
+        int s = 0;
+        int64_t k = 0;
+        BlockDesc next{};
+        if (int64_t(blockIdx.x) < M.nblk) next = load_desc(M.desc + blockIdx.x);
+        for (int64_t b = blockIdx.x; b < M.nblk; b += gridDim.x, ++k) {
+            const BlockDesc d = next;
+            if (b + gridDim.x < M.nblk) next = load_desc(M.desc + b + gridDim.x);
+            if (k >= STAGES) {
+                if (!mbar_wait_bounded(&sm.empty[s], (empty_par >> s) & 1u)) {
+                    atomicOr(err, kErrWaitTimeout);
+                    ok = false;
+                    break;
+                }
+                empty_par ^= 1u << s;
+            }
+            spmv_issue<V, X, A, TILE, STAGES>(M, x, d, sm, s);
+            full_par ^= 1u << s;
+            used |= 1u << s;
+            s = (s + 1 == STAGES) ? 0 : s + 1;
+        }
+        // Drain: every stage's last copy has landed before the CTA may exit.
+        for (int q = 0; q < STAGES; ++q)
+            if (used & (1u << q)) mbar_wait_bounded(&sm.full[q], ((full_par >> q) & 1u) ^ 1u);
+        return ok;
+    }
+
+    // ---- consumers ----
+    uint32_t full_par = 0;
     int s = 0;
     for (int64_t b = blockIdx.x; b < M.nblk; b += gridDim.x) {
-        const bool ok = mbar_wait_bounded(&sm.bar[s], (parity >> s) & 1u);
-        if (__syncthreads_or(!ok)) {
-            // Give up: report, then wait (bounded) for this CTA's copies still
-            // in flight so none lands in shared memory after exit.
-            if (t == 0) atomicOr(err, kErrWaitTimeout);
-            for (int q = 0; q < STAGES; ++q) {
-                const int sq = (s + q) % STAGES;
-                if (b + int64_t(q) * gridDim.x < M.nblk)
-                    mbar_wait_bounded(&sm.bar[sq], (parity >> sq) & 1u);
-            }
-            return false;
-        }
-        parity ^= 1u << s;
-        const int32_t z0 = sm.meta[s][2], z1 = sm.meta[s][3];
-        if (z1 - z0 > TILE) {
-            spmv_long_row<V, X, A, TILE, STAGES>(M, sm.meta[s][0], z0, z1, x, sm, epi);
-            __syncthreads();
+        const bool ok = mbar_wait_bounded(&sm.full[s], (full_par >> s) & 1u);
+        full_par ^= 1u << s;
+        bool good;
+        if (!ok || sm.meta[s].rz.w - sm.meta[s].rz.z <= TILE) {
+            good = spmv_tile<V, X, A, TILE, STAGES>(M, s, ok, x, sm, epi);
         } else {
-            spmv_tile<V, X, A, TILE, STAGES>(M, s, x, sm, epi);  // ends with a barrier
+            good = !consumer_sync_or(false);
+            if (good)
+                spmv_long_row<V, X, A, TILE, STAGES>(M, sm.meta[s].rz.x, sm.meta[s].rz.z,
+                                                     sm.meta[s].rz.w, x, sm, epi);
         }
-        // stage s and meta[s] are free again
-        if (t == 0) {
-            const int64_t nb = b + int64_t(STAGES) * gridDim.x;
-            if (nb < M.nblk) {
-                fence_proxy_async_smem();  // products were written over stage s
-                spmv_issue<V, A, TILE, STAGES>(M, next_desc, sm, s);
-                const int64_t nn = nb + gridDim.x;
-                if (nn < M.nblk) next_desc = __ldg(M.desc + nn);
-            }
+        if (!good) {
+            if (t == 0) atomicOr(err, kErrWaitTimeout);
+            return false;  // the producer drains its copies
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.empty[s]);  // this warp is done with stage s
         s = (s + 1 == STAGES) ? 0 : s + 1;
     }
     return true;
@@ -264,9 +380,9 @@ struct StoreEpi {
 };
 
 // Dynamic shared memory of the pipelined kernels.
-template <typename V, typename A, int TILE, int STAGES>
+template <typename V, typename X, typename A, int TILE, int STAGES>
 constexpr size_t spmv_smem_bytes() {
-    return sizeof(SpmvSmem<V, A, TILE, STAGES>);
+    return sizeof(SpmvSmem<V, X, A, TILE, STAGES>);
 }
 
 }  // namespace nm

@@ -193,3 +193,51 @@ def test_argument_errors(kspmv):
         kspmv.spmv(M, torch.zeros(4, dtype=torch.float64), good)
     with pytest.raises(ValueError, match="contiguous"):
         kspmv.spmv(M, torch.zeros(8, dtype=torch.float64, device="cuda")[::2], good)
+
+
+@pytest.mark.parametrize("tile,stages", [(1024, 2), (1024, 3), (2048, 2), (2048, 3), (4096, 2)])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_staged_x_windows_and_fallback(kspmv, oracle, tile, stages, aligned):
+    # Stencil blocks stage their x windows (TMA) when x is 16-byte aligned; an
+    # x that starts 8 bytes into an allocation must take the gather path.
+    # Both must equal the serial oracle bit for bit (all rows thread-reduced).
+    A = gen.laplacian_3d(48)
+    x = np.random.default_rng(tile + stages).uniform(-1, 1, A.ncols)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    kspmv.tune(M, tile=tile, stages=stages)
+    buf = torch.zeros(A.ncols + 1, dtype=torch.float64, device="cuda")
+    xt = buf[1:] if not aligned else buf[:-1]
+    xt.copy_(torch.tensor(x))
+    assert (xt.data_ptr() % 16 == 0) == aligned
+    yt = torch.full((A.nrows,), float("nan"), dtype=torch.float64, device="cuda")
+    kspmv.spmv(M, xt, yt)
+    assert np.array_equal(yt.cpu().numpy(), oracle.spmv(A.row_ptr, A.col_idx, A.values, x))
+
+
+@pytest.mark.parametrize("tile", [1024, 2048])
+def test_staged_x_ragged_columns(kspmv, oracle, tile):
+    # Rows whose columns fall in a few narrow bands (staged) mixed with rows of
+    # random columns (too many windows: gathered), odd ncols (the last block's
+    # windows would pass the end of x, so it must gather), FP64 and FP32.
+    rng = np.random.default_rng(tile)
+    n, ncols = 20_000, 20_003
+    rows = []
+    for i in range(n):
+        if (i // 300) % 2 == 0:
+            base = [i, (i * 7) % (ncols - 40), ncols - 1 - (i % 37)]
+            c = np.unique(np.concatenate([b + np.arange(-3, 4) for b in base]))
+            c = c[(c >= 0) & (c < ncols)]
+        else:
+            c = np.unique(rng.integers(0, ncols, rng.integers(1, 12)))
+        rows.append(c)
+    rp = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    ci = np.concatenate(rows).astype(np.int32)
+    A = gen.Csr(rp, ci, rng.standard_normal(rp[-1]), n, ncols)
+    x = rng.uniform(-1, 1, ncols)
+    y, M = _run(kspmv, A, x, tuning={"tile": tile})
+    _check64(oracle, A, x, y, kspmv.row_blocks(M)[1])
+    y32, _ = _run(kspmv, A, x.astype(np.float32), precision="fp32", tuning={"tile": tile})
+    ref32 = oracle.spmv(A.row_ptr, A.col_idx, A.values.astype(np.float32), x.astype(np.float32))
+    scale = oracle.spmv(A.row_ptr, A.col_idx, np.abs(A.values).astype(np.float32),
+                        np.abs(x).astype(np.float32))
+    assert np.all(np.abs(y32 - ref32) <= TOL32 * scale)
