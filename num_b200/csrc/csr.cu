@@ -170,7 +170,7 @@ int rebuild_blocks(nm_csr* A) {
                 d.xs = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
                 d.xl = make_int4(0, 0, 0, 0);
             } else {
-                block_xwindows(ci, z0, z1, ncols, tile, scratch, &d.xs, &d.xl);
+                block_xwindows(ci, z0, z1, ncols, xwin_capacity(tile), scratch, &d.xs, &d.xl);
             }
         }
     };

@@ -30,6 +30,8 @@ struct CgWorkspace;  // cg.cu
 // multiple of 4 elements, that together hold every column the block's
 // nonzeros reference; the SpMV kernels stage them with the block's nonzeros.
 constexpr int kXSeg = 4;
+// Elements of x a block of a TILE-nonzero partition may stage.
+__host__ __device__ constexpr int xwin_capacity(int tile) { return tile / 2 + 384; }
 constexpr int kXGap = 16;  // gaps up to this many elements are bridged
 struct BlockDesc {
     int4 rz;

@@ -10,17 +10,17 @@
 //    counts the transaction bytes, an `empty` mbarrier per stage counts the
 //    consumer warps that have released it, so the producer runs up to STAGES
 //    blocks ahead of the consumers;
-//  * eight consumer warps (256 threads, named barrier 1) compute the block:
-//    every thread multiplies staged values with the staged x window entries
-//    (x[col] from global memory when the block has no windows), writes the
-//    products back over the staged operands, and rows with <= short_max
+//  * eight consumer warps (256 threads, named barrier 1) compute the block
+//    from the staged operands and the staged x window entries (x[col] from
+//    global memory when the block has no windows): rows with <= short_max
 //    nonzeros are summed by one thread each, serially in CSR order
 //    (bit-identical to the reference's serial row loop,
 //    src/spmv_kernel.hpp:90-97); longer rows by one warp each.  A block that
 //    is one row with more than TILE nonzeros is read straight from global
 //    memory by all consumers and reduced with a deterministic sum.
 //
-// A block without warp rows costs the consumers one named barrier.
+// A block without warp rows costs the consumers no barrier at all: each warp
+// releases the stage on its own.
 //
 // The epilogue functor receives (row, value) exactly once per row, on one
 // consumer thread; CG uses it to store Ap and to accumulate p.Ap on the fly.
@@ -33,8 +33,10 @@
 // 16-byte aligned.
 //
 // Every mbarrier wait is bounded (mbar_wait_bounded).  When one gives up the
-// kernel sets the device error word, the consumers stop, and the producer
-// waits (bounded again) for its copies still in flight before the CTA exits.
+// kernel sets the device error word; that consumer stops waiting and stops
+// touching staged data (but keeps the CTA's barrier schedule), and the
+// producer waits (bounded again) for its copies still in flight before the
+// CTA exits.
 #pragma once
 
 #include "csr.cuh"
@@ -88,7 +90,7 @@ struct alignas(16) SpmvStage {
     int32_t col[TILE + 16];
     V val[TILE + 16];
     int32_t rp[kThreads + 8];
-    X xw[TILE];  // the block's x windows, back to back
+    X xw[xwin_capacity(TILE)];  // the block's x windows, back to back
 };
 
 template <typename V, typename X, typename A, int TILE, int STAGES>
@@ -101,16 +103,6 @@ struct SpmvSmem {
     int32_t warp_cnt[kWarps];
     A red[kWarps + 1];
 };
-
-// Product storage: over the staged values when they are as wide as the
-// accumulator, else over the staged column indices (bf16 values, float
-// products).  Each slot is read by the thread that then overwrites it.
-template <typename V, typename X, typename A, int TILE>
-__device__ __forceinline__ A* prod_slots(SpmvStage<V, X, TILE>& st) {
-    static_assert(sizeof(A) == sizeof(V) || sizeof(A) == sizeof(int32_t), "product slot");
-    if constexpr (sizeof(A) == sizeof(V)) return reinterpret_cast<A*>(st.val);
-    else return reinterpret_cast<A*>(st.col);
-}
 
 __device__ __forceinline__ BlockDesc load_desc(const BlockDesc* p) {
     const int4* q = reinterpret_cast<const int4*>(p);
@@ -167,12 +159,12 @@ __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restr
 
 // One long row (nnz > TILE) straight from global memory, all consumers.
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
-__device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, int32_t r0, int32_t z0,
-                                              int32_t z1, const X* __restrict__ x,
+__device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int32_t r0,
+                                              int32_t z0, int32_t z1, const X* __restrict__ x,
                                               SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
     const int t = threadIdx.x;
     A s = A(0);
-    for (int32_t j = (z0 & ~3) + 4 * t; j < z1; j += 4 * kConsumers) {
+    for (int32_t j = (z0 & ~3) + 4 * t; ok && j < z1; j += 4 * kConsumers) {
         const int4 c = ld_stream(reinterpret_cast<const int4*>(M.col_idx + j));
         A v[4];
         Load4<V, A>::run(M.values, j, v);
@@ -184,89 +176,64 @@ __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, int32_t r0, i
         }
     }
     s = consumer_sum(s, sm.red);
-    if (t == 0) epi(r0, s);
+    if (t == 0 && ok) epi(r0, s);
 }
 
-// Consumers: one staged multi-row block.  `ok` = this thread saw the stage
-// complete.  Returns false (uniformly) if any consumer did not.
+// Consumers: one staged multi-row block, straight from the staged operands.
+// A row with <= short_max nonzeros is summed by one thread serially in CSR
+// order; longer rows by a warp.  `ok` = this thread saw the stage complete;
+// a thread that did not touches no staged data but takes the same barriers
+// (the control flow depends only on the descriptor d).
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
-__device__ __forceinline__ bool spmv_tile(const CsrView<V>& M, int s, bool ok,
+__device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, const BlockDesc& d,
                                           const X* __restrict__ x,
                                           SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
-    SpmvStage<V, X, TILE>& st = sm.st[s];
-    A* prod = prod_slots<V, X, A, TILE>(st);
-    if (ok) {
-        const BlockDesc d = sm.meta[s];
-        const int32_t z0 = d.rz.z, z1 = d.rz.w;
-        const int32_t a0 = z0 & ~7;
-        const int cnt = z1 - a0;
-        // column -> staged x slot: window k holds columns [xs_k, xs_k + xl_k)
-        const bool staged = d.xs.x >= 0;
-        const int32_t dl0 = -d.xs.x, dl1 = d.xl.x - d.xs.y, dl2 = d.xl.x + d.xl.y - d.xs.z,
-                      dl3 = d.xl.x + d.xl.y + d.xl.z - d.xs.w;
-        // every x read of this thread is issued before any product is formed
-        constexpr int kPer = (TILE + 16 + kConsumers - 1) / kConsumers;
-        const int e0 = (z0 - a0) + t;
-        int c[kPer];
-        A v[kPer];
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int e = e0 + q * kConsumers;
-            c[q] = e < cnt ? st.col[e] : -1;
-            v[q] = e < cnt ? widen<V, A>(st.val[e]) : A(0);
-        }
-        A xv[kPer];
-        if (staged) {
-#pragma unroll
-            for (int q = 0; q < kPer; ++q) {
-                const int32_t cq = c[q];
-                const int32_t dl =
-                    cq >= d.xs.w ? dl3 : (cq >= d.xs.z ? dl2 : (cq >= d.xs.y ? dl1 : dl0));
-                xv[q] = cq >= 0 ? static_cast<A>(st.xw[cq + dl]) : A(0);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kPer; ++q)
-                xv[q] = c[q] >= 0 ? static_cast<A>(__ldg(x + c[q])) : A(0);
-        }
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int e = e0 + q * kConsumers;
-            if (e < cnt) prod[e] = mul_rn(v[q], xv[q]);
-        }
-        // products overwrite staged operands that the next TMA copy into this
-        // stage will overwrite again: order them before that copy
-        fence_proxy_async_smem();
-    }
-    if (consumer_sync_or(!ok)) return false;  // products visible; all saw the stage
-
-    const BlockDesc d = sm.meta[s];
-    const int32_t r0 = d.rz.x, r1 = d.rz.y, z0 = d.rz.z;
-    const int nr = r1 - r0;
+    const SpmvStage<V, X, TILE>& st = sm.st[s];
+    const int32_t r0 = d.rz.x, z0 = d.rz.z;
+    const int nr = d.rz.y - r0;
     const int32_t a0 = z0 & ~7;
     const int32_t roff = r0 - (r0 & ~3);  // row r0's slot in the staged row_ptr
+    // column -> staged x slot: window k holds columns [xs_k, xs_k + xl_k)
+    const bool staged = d.xs.x >= 0;
+    const int32_t dl0 = -d.xs.x, dl1 = d.xl.x - d.xs.y, dl2 = d.xl.x + d.xl.y - d.xs.z,
+                  dl3 = d.xl.x + d.xl.y + d.xl.z - d.xs.w;
+    auto xval = [&](int32_t c) -> A {
+        if (staged) {
+            const int32_t dl = c >= d.xs.w ? dl3 : (c >= d.xs.z ? dl2 : (c >= d.xs.y ? dl1 : dl0));
+            return static_cast<A>(st.xw[c + dl]);
+        }
+        return static_cast<A>(__ldg(x + c));
+    };
 
-    // thread-per-row reduction
     bool is_long = false;
-    if (t < nr) {
+    if (ok && t < nr) {
         const int32_t s0 = st.rp[roff + t] - a0, s1 = st.rp[roff + t + 1] - a0;
         if (s1 - s0 <= M.short_max) {
-            // serial CSR-order sum; loads batched four at a time
+            // serial CSR-order sum, operands fetched four at a time
             A acc = A(0);
             int32_t j = s0;
             for (; j + 4 <= s1; j += 4) {
-                const A p0 = prod[j], p1 = prod[j + 1], p2 = prod[j + 2], p3 = prod[j + 3];
-                acc = add_rn(add_rn(add_rn(add_rn(acc, p0), p1), p2), p3);
+                int32_t c[4];
+                A v[4], xv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    c[q] = st.col[j + q];
+                    v[q] = widen<V, A>(st.val[j + q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) xv[q] = xval(c[q]);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc = add_rn(acc, mul_rn(v[q], xv[q]));
             }
-            for (; j < s1; ++j) acc = add_rn(acc, prod[j]);
+            for (; j < s1; ++j) acc = add_rn(acc, mul_rn(widen<V, A>(st.val[j]), xval(st.col[j])));
             epi(r0 + t, acc);
         } else {
             is_long = true;
         }
     }
-    if (d.aux.x == 0) return true;  // no warp rows in this block
+    if (d.aux.x == 0) return;  // no warp rows in this block
 
     // deterministic list of long rows in row order (ballot + warp prefix)
     const unsigned m = __ballot_sync(0xffffffffu, is_long);
@@ -285,13 +252,17 @@ __device__ __forceinline__ bool spmv_tile(const CsrView<V>& M, int s, bool ok,
     // warp-per-row reduction of the long rows
     for (int q = warp; q < nl; q += kWarps) {
         const int tt = sm.long_rows[q];
-        const int32_t s0 = st.rp[roff + tt] - a0, s1 = st.rp[roff + tt + 1] - a0;
         A acc = A(0);
-        for (int32_t j = s0 + lane; j < s1; j += 32) acc += prod[j];
+        if (ok) {
+            const int32_t s0 = st.rp[roff + tt] - a0, s1 = st.rp[roff + tt + 1] - a0;
+            for (int32_t j = s0 + lane; j < s1; j += 32)
+                acc += mul_rn(widen<V, A>(st.val[j]), xval(st.col[j]));
+        }
         acc = warp_sum(acc);
-        if (lane == 0) epi(r0 + tt, acc);
+        if (lane == 0 && ok) epi(r0 + tt, acc);
     }
-    return true;
+    // long_rows / warp_cnt are next written after a consumer barrier of a later
+    // block, which every warp reaches only after leaving this loop.
 }
 
 // The persistent pipelined loop over this CTA's row blocks, for all 288
@@ -347,29 +318,31 @@ __device__ __forceinline__ bool spmv_pipeline(const CsrView<V>& M, const X* __re
     }
 
     // ---- consumers ----
+    // A consumer whose bounded wait gave up stops touching staged data and
+    // waiting, but keeps taking the same barriers until the loop ends.
     uint32_t full_par = 0;
+    bool failed = false;
     int s = 0;
     for (int64_t b = blockIdx.x; b < M.nblk; b += gridDim.x) {
-        const bool ok = mbar_wait_bounded(&sm.full[s], (full_par >> s) & 1u);
+        bool ok = false;
+        if (!failed) {
+            ok = mbar_wait_bounded(&sm.full[s], (full_par >> s) & 1u);
+            if (!ok) {
+                failed = true;
+                atomicOr(err, kErrWaitTimeout);
+            }
+        }
         full_par ^= 1u << s;
-        bool good;
-        if (!ok || sm.meta[s].rz.w - sm.meta[s].rz.z <= TILE) {
-            good = spmv_tile<V, X, A, TILE, STAGES>(M, s, ok, x, sm, epi);
-        } else {
-            good = !consumer_sync_or(false);
-            if (good)
-                spmv_long_row<V, X, A, TILE, STAGES>(M, sm.meta[s].rz.x, sm.meta[s].rz.z,
-                                                     sm.meta[s].rz.w, x, sm, epi);
-        }
-        if (!good) {
-            if (t == 0) atomicOr(err, kErrWaitTimeout);
-            return false;  // the producer drains its copies
-        }
+        const BlockDesc d = ok ? sm.meta[s] : load_desc(M.desc + b);
+        if (d.rz.w - d.rz.z > TILE)
+            spmv_long_row<V, X, A, TILE, STAGES>(M, ok, d.rz.x, d.rz.z, d.rz.w, x, sm, epi);
+        else
+            spmv_rows<V, X, A, TILE, STAGES>(M, s, ok, d, x, sm, epi);
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.empty[s]);  // this warp is done with stage s
         s = (s + 1 == STAGES) ? 0 : s + 1;
     }
-    return true;
+    return !failed;
 }
 
 // Epilogue: y[row] = value.
