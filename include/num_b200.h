@@ -117,6 +117,22 @@ int nm_csr_info(const nm_csr* A, int32_t* nrows, int32_t* ncols, int32_t* nnz,
 int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t);
 int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t);
 
+/* One timed candidate of nm_csr_autotune. */
+typedef struct {
+    nm_tuning tuning;
+    float us;  /* average device time of one SpMV under `tuning` */
+} nm_tune_trial;
+
+/* SpMV autotuner (no reference counterpart; the reference's partition is
+ * fixed).  Times y = A*x on `stream` under every candidate tile (1024, 2048,
+ * 4096), short_max (32, 64), stages (2, 3, 4; those whose shared memory fits)
+ * and grid_mult (0, 1, 2), spending about budget_ms of device time (<= 0:
+ * 200 ms), installs the fastest on A and returns it in *best.  x is read; y
+ * is overwritten.  trials[0..min(cap, *ntrials)) receive every timing (trials
+ * may be NULL when cap is 0).  Synchronises `stream`. */
+int nm_csr_autotune(nm_csr* A, const void* x, void* y, void* stream, double budget_ms,
+                    nm_tuning* best, nm_tune_trial* trials, int32_t cap, int32_t* ntrials);
+
 /* Copies the row-block boundaries (nblocks+1 entries) and, if bins != NULL,
  * the per-row reduction bin (0 thread, 1 warp, 2 CTA) to host memory. */
 int nm_csr_row_blocks(const nm_csr* A, int32_t* blk, int32_t cap, int8_t* bins);
@@ -184,6 +200,74 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * callers and synchronises `stream` before returning. */
 int nm_cg_local_static(const nm_csr* A, const double* b, double* x, double tol,
                        int32_t max_iter, nm_cg_result* result, void* stream);
+
+/* ---- batched / mixed-precision / served solver (no counterpart in the reference) */
+
+typedef struct nm_solver nm_solver;
+
+/* Solver options.  inner: value precision of the inner iterations -- NM_F64
+ * (plain FP64 Jacobi-PCG, no refinement), NM_F32 or NM_BF16 (FP32 vectors and
+ * accumulation, FP64 iterative refinement).  precond: 1 Jacobi, 0 none.
+ * inner_rtol: relative reduction of one inner solve (default 1e-4; ignored
+ * for NM_F64).  max_outer: refinement steps before giving up (default 30). */
+typedef struct {
+    int32_t inner;
+    int32_t precond;
+    double inner_rtol;
+    int32_t max_outer;
+} nm_solver_opts;
+
+/* A solver with a device arena for up to max_rows rows and max_nnz nonzeros
+ * in total over max_systems concurrently resident systems. */
+int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_systems,
+                     const nm_solver_opts* opts, nm_solver** out);
+int nm_solver_destroy(nm_solver* S);
+
+/* Admit one SPD system A x = b (host CSR, FP64; x0 may be NULL for zero) with
+ * its own tolerance |b - A x| / |b| < tol and iteration cap.  Returns
+ * NM_ERR_NOMEM when its rows or nonzeros do not fit the free arena or no
+ * slot is free (admission by free device memory); *slot identifies it. */
+int nm_solver_admit(nm_solver* S, const int32_t* row_ptr, const int32_t* col_idx,
+                    const double* values, int32_t n, const double* b, const double* x0,
+                    double tol, int32_t max_iter, int32_t* slot);
+
+/* Admit systems in order, preparing them in parallel on the host, until one
+ * does not fit (FIFO): *admitted = how many were admitted, slots[0..admitted)
+ * their slots.  Returns NM_OK when the rest merely did not fit. */
+int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t* const* row_ptr,
+                          const int32_t* const* col_idx, const double* const* values,
+                          const int32_t* n, const double* const* b, double tol, int32_t max_iter,
+                          int32_t* slots, int32_t* admitted);
+
+/* One step of the batch: the pending refinement steps, then `iters` inner
+ * iterations of every active system, then the systems' states are read back;
+ * *n_done = systems that finished in this step.  Synchronous. */
+int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done);
+
+/* Engine counters since creation: steps run, list rebuilds, chunk graph
+ * captures and full instantiations, outer (refinement) launches, inner
+ * iterations enqueued, and host seconds spent per part of nm_solver_step
+ * (list upload, outer launch, capture, graph run + state read-back, state
+ * scan). */
+typedef struct {
+    int64_t steps, list_uploads, graph_captures, graph_instantiations, outer_launches,
+        inner_iterations;
+    double s_lists, s_outer, s_capture, s_run, s_scan;
+} nm_solver_counters;
+int nm_solver_counters_get(const nm_solver* S, nm_solver_counters* out);
+
+/* State of a slot: phase (1 refining, 2 iterating, 3 done), result (iters =
+ * inner iterations, final_res = |b - A x| / |b| of the last refinement
+ * step), refinement steps taken. */
+int nm_solver_status(const nm_solver* S, int32_t slot, int32_t* phase, nm_cg_result* result,
+                     int32_t* outer);
+
+/* Copy the solution to host memory (x_host may be NULL) and free the slot. */
+int nm_solver_take(nm_solver* S, int32_t slot, double* x_host);
+
+/* Largest free row and nonzero ranges, active systems, free slots. */
+int nm_solver_info(const nm_solver* S, int64_t* free_rows, int64_t* free_nnz, int32_t* active,
+                   int32_t* free_slots);
 
 /* ---- distributed slice, halo pack / unpack -------------------------------- */
 

@@ -26,9 +26,25 @@ class CgResult(C.Structure):
     _fields_ = [("iters", C.c_int32), ("final_res", C.c_double), ("converged", C.c_int32)]
 
 
+class SolverOpts(C.Structure):
+    _fields_ = [("inner", C.c_int32), ("precond", C.c_int32), ("inner_rtol", C.c_double),
+                ("max_outer", C.c_int32)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("tile", C.c_int32), ("max_rows", C.c_int32), ("short_max", C.c_int32),
                 ("grid_mult", C.c_int32), ("stages", C.c_int32)]
+
+
+class SolverCounters(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("steps", "list_uploads", "graph_captures",
+                                         "graph_instantiations", "outer_launches",
+                                         "inner_iterations")] + \
+               [(n, C.c_double) for n in ("s_lists", "s_outer", "s_capture", "s_run", "s_scan")]
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("tuning", Tuning), ("us", C.c_float)]
 
 
 # name -> (argtypes); every function returns int (nm_status) unless noted.
@@ -44,6 +60,7 @@ _SIGNATURES = {
     "nm_csr_info": ([vp, P_i32, P_i32, P_i32, P_i32, P_i32], C.c_int),
     "nm_csr_set_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
     "nm_csr_get_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
+    "nm_csr_autotune": ([vp, vp, vp, vp, C.c_double, C.POINTER(Tuning), vp, i32, P_i32], C.c_int),
     "nm_csr_row_blocks": ([vp, vp, i32, vp], C.c_int),
     "nm_row_blocks_host": ([vp, i32, C.POINTER(Tuning), vp, i32, vp, P_i32], C.c_int),
     "nm_spmv": ([vp, vp, vp, vp], C.c_int),
@@ -57,6 +74,15 @@ _SIGNATURES = {
     "nm_scale": ([i64, dbl, vp, vp], C.c_int),
     "nm_cg_local": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
     "nm_cg_local_static": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
+    "nm_solver_create": ([i64, i64, i32, C.POINTER(SolverOpts), C.POINTER(vp)], C.c_int),
+    "nm_solver_destroy": ([vp], C.c_int),
+    "nm_solver_admit": ([vp, vp, vp, vp, i32, vp, vp, dbl, i32, P_i32], C.c_int),
+    "nm_solver_admit_batch": ([vp, i32, vp, vp, vp, vp, vp, dbl, i32, P_i32, P_i32], C.c_int),
+    "nm_solver_step": ([vp, i32, P_i32], C.c_int),
+    "nm_solver_counters_get": ([vp, vp], C.c_int),
+    "nm_solver_status": ([vp, i32, P_i32, C.POINTER(CgResult), P_i32], C.c_int),
+    "nm_solver_take": ([vp, i32, vp], C.c_int),
+    "nm_solver_info": ([vp, C.POINTER(i64), C.POINTER(i64), P_i32, P_i32], C.c_int),
     "nm_dist_create": ([vp, vp, vp, i32, i32, i32, i32, C.POINTER(vp)], C.c_int),
     "nm_dist_destroy": ([vp], C.c_int),
     "nm_dist_plan": ([vp, vp, vp, i32, i32, i32, i32, C.POINTER(vp)], C.c_int),

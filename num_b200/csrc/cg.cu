@@ -71,6 +71,7 @@ struct PApEpi {
         Ap[row] = v;
         dot = fma(__ldg(p + row), v, dot);
     }
+    __device__ __forceinline__ void end_block(int64_t, const BlockDesc&, double (*)[kWarps]) {}
 };
 
 template <int TILE, int STAGES>

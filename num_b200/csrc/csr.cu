@@ -46,8 +46,27 @@ void block_xwindows(const int32_t* ci, int32_t z0, int32_t z1, int32_t ncols, in
     *xs = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
     *xl = make_int4(0, 0, 0, 0);
     if (z1 <= z0) return;
-    c.assign(ci + z0, ci + z1);
-    std::sort(c.begin(), c.end());
+    int32_t cmin = ci[z0], cmax = ci[z0];
+    for (int32_t j = z0 + 1; j < z1; ++j) {
+        cmin = std::min(cmin, ci[j]);
+        cmax = std::max(cmax, ci[j]);
+    }
+    const int64_t span = int64_t(cmax) - cmin + 1;
+    if (span <= 64 * int64_t(z1 - z0)) {
+        // narrow range: mark the columns in a bitmap, read them back in order
+        std::vector<uint64_t> bits(size_t((span + 63) / 64), 0);
+        for (int32_t j = z0; j < z1; ++j) {
+            const int64_t o = ci[j] - cmin;
+            bits[size_t(o >> 6)] |= uint64_t(1) << (o & 63);
+        }
+        c.clear();
+        for (size_t w = 0; w < bits.size(); ++w)
+            for (uint64_t m = bits[w]; m; m &= m - 1)
+                c.push_back(cmin + int32_t(w * 64 + size_t(__builtin_ctzll(m))));
+    } else {
+        c.assign(ci + z0, ci + z1);
+        std::sort(c.begin(), c.end());
+    }
     int32_t st[kXSeg], en[kXSeg];
     int nseg = 0;
     int32_t cs = c[0] & ~3, ce = (c[0] | 3) + 1;
@@ -147,6 +166,8 @@ int upload(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals) {
     return NM_OK;
 }
 
+}  // namespace
+
 int rebuild_blocks(nm_csr* A) {
     std::vector<int32_t> blk;
     A->nblk = build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
@@ -201,6 +222,8 @@ int rebuild_blocks(nm_csr* A) {
     return NM_OK;
 }
 
+namespace {
+
 int finish_create(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals,
                   nm_csr** out) {
     int st = upload(A, rp, ci, vals);
@@ -218,6 +241,11 @@ int finish_create(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* v
 }
 
 }  // namespace
+
+void reset_cg(nm_csr* A) {
+    std::lock_guard<std::mutex> lock(A->cg_mutex);
+    A->cg.reset();
+}
 
 int spmv_grid(const nm_csr* A, int ctas_per_sm) {
     // Persistent grid: every CTA that fits (or grid_mult per SM when set).

@@ -37,7 +37,7 @@ struct BlockDesc {
     int4 rz;
     int4 xs;
     int4 xl;
-    int4 aux;  // {rows reduced by a warp (nnz > short_max), 0, 0, 0}
+    int4 aux;  // {rows reduced by a warp (nnz > short_max), system slot, 0, 0}
 };
 
 // Kernel-side view of a matrix.
@@ -51,6 +51,7 @@ struct CsrView {
     int32_t nrows;
     int32_t short_max;
     int32_t stage_x;  // 1: x windows are staged (x 16-byte aligned); 0: gather from global
+    const int32_t* nblk_dev;  // when set, the block count is read from device memory
 };
 
 // Default row-block parameters.
@@ -94,7 +95,7 @@ struct nm_csr {
     nm::CsrView<V> view() const {
         return nm::CsrView<V>{d_row_ptr, d_col_idx, static_cast<const V*>(d_values),
                               d_desc,    nblk,      nrows,
-                              tune.short_max, 0};
+                              tune.short_max, 0, nullptr};
     }
 };
 
@@ -103,4 +104,11 @@ namespace nm {
 int spmv_grid(const nm_csr* A, int ctas_per_sm);
 // Launches y = A*x on `stream` (dtype-dispatched).  Used by the API and CG.
 int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t stream);
+// Dynamic shared memory of the SpMV kernel for (dtype, tile, stages); 0 if
+// the combination does not exist.
+size_t spmv_smem_for(int dtype, int tile, int stages);
+// Rebuilds the row-block partition and descriptors of A under A->tune.
+int rebuild_blocks(nm_csr* A);
+// Drops A's cached CG workspace (its graphs hold the current descriptors).
+void reset_cg(nm_csr* A);
 }  // namespace nm

@@ -1,0 +1,1340 @@
+// solver.cu -- batched, mixed-precision, continuously batched PCG engine.
+//
+// No counterpart in the reference (its CG solves one system at a time, in
+// FP64, without a preconditioner, src/cg_solver.hpp:133-196).  Design:
+//
+// * Arena.  Every admitted system lives in one device arena: row-indexed
+//   vectors (b, x, r64 in FP64; p, Ap, r, z, d, Jacobi inverse diagonal in the
+//   inner precision T) and nonzero-indexed CSR arrays (column indices stored
+//   as arena rows, FP64 values for the outer residual, inner-precision values
+//   for the inner iterations).  The active systems therefore form one
+//   block-diagonal matrix, and the pipelined SpMV kernel of spmv.cuh runs over
+//   a list of the active systems' row blocks.  Admission takes first-fit
+//   ranges of rows and nonzeros and fails (NM_ERR_NOMEM) when the arena is
+//   full: admission by free device memory.
+//
+// * Lockstep iterations.  Every inner iteration advances all active systems
+//   with per-system scalars:  SpMV + per-warp partials of p.Ap  ->  per-system
+//   alpha  ->  d += alpha p, r -= alpha Ap, z = M^-1 r, partials of r.z and
+//   r.r  ->  per-system beta and inner stopping test  ->  p = z + beta p.
+//   Systems that stop are gated out of the SpMV and skipped by the vector
+//   kernels; all grids are persistent, list lengths are read from device
+//   memory.
+//
+// * Mixed precision with iterative refinement.  The inner Jacobi-PCG runs in
+//   T = float (values float or bf16, FP32 accumulation) on the scaled
+//   residual system A d = r64 / |r64|; an outer step (x += d |r64|,
+//   r64 = b - A x with FP64 values, fused into the FP64 SpMV's epilogue,
+//   |r64| / |b|) runs between chunks for systems whose inner solve stopped,
+//   until |b - A x| / |b| < tol.  With T = double the same machinery is a
+//   plain FP64 PCG (the inner test is the final one).
+//
+// * Continuous batching.  nm_solver_step runs the pending outer steps, then a
+//   chunk of inner iterations, then reads every system's state; the host
+//   admits new systems and retires finished ones between steps.
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "spmv.cuh"
+
+namespace nm {
+
+enum SysPhase : int32_t { kSysFree = 0, kSysOuter = 1, kSysInner = 2, kSysDone = 3 };
+
+struct SysState {
+    // set at admission
+    int32_t row0, n, max_iter, max_outer;
+    double tol, bnorm, inner_rtol, stop_frac;
+    // dynamic
+    int32_t phase, it_total, it_inner, outer;
+    int32_t converged, pad_;
+    double rnorm, rz, rr0, rr, alpha, beta, final_res;
+};
+
+struct SysRef {
+    int32_t slot, blk0, blk1, tile0, tile1, pad_[3];
+};
+
+// Counts of the device-side work lists.
+struct ListHdr {
+    int32_t iblk, itile, isys, oblk, otile, osys, pad_[2];
+};
+
+constexpr int kTileRows = 1024;  // rows per vector-kernel tile (within one system)
+
+__device__ __forceinline__ int32_t sys_phase(const SysState* sys, int32_t slot) {
+    return __ldcg(&sys[slot].phase);
+}
+
+// ---- SpMV epilogues / gates ---------------------------------------------------
+
+// Sum of part[lo, hi) by one warp in a fixed order (lane-strided, 8
+// independent accumulators by relative index, then the shuffle tree): the
+// same grouping wherever the range sits; valid in every lane.
+__device__ __forceinline__ double warp_ordered_sum(const double* part, int64_t lo, int64_t hi) {
+    const int lane = threadIdx.x & 31;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t i = lo + lane;
+    for (; i + 7 * 32 < hi; i += 8 * 32) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldcg(part + i + k * 32);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] += v[k];
+    }
+    for (int k = 0; i < hi; i += 32, ++k) a[k] += __ldcg(part + i);
+    double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+// Ap = A p.  Per block: the sum of p.Ap over its rows; the warp whose block
+// arrives last for its system sums that system's block sums in block order
+// and sets alpha = r.z / p.Ap.
+template <typename T>
+struct InnerEpi {
+    T* __restrict__ Ap;
+    const T* __restrict__ p;
+    double* __restrict__ part;
+    unsigned int* __restrict__ cnt;  // per slot: blocks arrived this launch
+    const int2* __restrict__ sblk;   // per slot: its block range in the list
+    SysState* sys;
+    T acc;
+    __device__ __forceinline__ void operator()(int32_t row, T v) {
+        Ap[row] = v;
+        acc += __ldg(p + row) * v;
+    }
+    __device__ __forceinline__ void end_block(int64_t b, const BlockDesc& d,
+                                              double (*buf)[kWarps]) {
+        consumer_block_sum(double(acc), buf, b, part + b);
+        acc = T(0);
+        if ((threadIdx.x >> 5) != 0) return;  // warp 0 finalises
+        const int lane = threadIdx.x & 31;
+        const int32_t slot = d.aux.y;
+        const int2 range = __ldg(sblk + slot);
+        int last = 0;
+        if (lane == 0) {
+            __threadfence();  // this block's sum before the arrival
+            last = atomicAdd(cnt + slot, 1u) == unsigned(range.y - range.x - 1);
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) return;
+        __threadfence();
+        const double pAp = warp_ordered_sum(part, range.x, range.y);
+        if (lane == 0) {
+            cnt[slot] = 0u;
+            SysState& S = sys[slot];
+            if (S.phase == kSysInner) S.alpha = (pAp != 0.0) ? S.rz / pAp : 0.0;
+        }
+    }
+};
+
+struct OuterEpi {  // r64 = b - A x, per-warp partials of r64.r64
+    double* __restrict__ r64;
+    const double* __restrict__ b;
+    double* __restrict__ part;
+    double acc;
+    __device__ __forceinline__ void operator()(int32_t row, double v) {
+        const double r = __ldg(b + row) - v;
+        r64[row] = r;
+        acc = fma(r, r, acc);
+    }
+    __device__ __forceinline__ void end_block(int64_t b, const BlockDesc&,
+                                              double (*buf)[kWarps]) {
+        consumer_block_sum(acc, buf, b, part + b);
+        acc = 0.0;
+    }
+};
+
+struct PhaseGate {  // only blocks of systems in the given phase
+    const SysState* sys;
+    int32_t phase;
+    __device__ __forceinline__ bool operator()(const BlockDesc& d) const {
+        return sys_phase(sys, d.aux.y) == phase;
+    }
+};
+
+constexpr int kSolverTile = 2048;
+constexpr int kSolverStages = 2;
+
+template <typename V, typename T>
+__global__ void __launch_bounds__(kCtaThreads)
+    bs_spmv_inner(CsrView<V> M, const T* __restrict__ p, T* __restrict__ Ap, SysState* sys,
+                  double* part, unsigned int* cnt, const int2* sblk, unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<V, T, T, kSolverTile, kSolverStages>*>(smem_raw);
+    InnerEpi<T> epi{Ap, p, part, cnt, sblk, sys, T(0)};
+    spmv_pipeline<V, T, T, kSolverTile, kSolverStages>(M, p, sm, epi, err,
+                                                       PhaseGate{sys, kSysInner});
+}
+
+__global__ void __launch_bounds__(kCtaThreads)
+    bs_spmv_outer(CsrView<double> M, const double* __restrict__ x, const double* __restrict__ b,
+                  double* __restrict__ r64, const SysState* sys, double* part, unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm =
+        *reinterpret_cast<SpmvSmem<double, double, double, kSolverTile, kSolverStages>*>(smem_raw);
+    OuterEpi epi{r64, b, part, 0.0};
+    spmv_pipeline<double, double, double, kSolverTile, kSolverStages>(M, x, sm, epi, err,
+                                                                      PhaseGate{sys, kSysOuter});
+}
+
+// ---- per-system scalar steps -------------------------------------------------------
+
+enum ScalarKind { kOuterNorm = 2, kStart = 3 };
+
+constexpr int kScalarThreads = 1024;
+
+// Sum of part[lo, hi) (stride `step`, offset `off`) in a fixed order; valid in
+// thread 0.  Thread t owns the entries lo + t + k*blockDim (k = 0, 1, ...),
+// summed with 8 independent accumulators (entry k goes to accumulator k % 8)
+// that are then added in order -- the same grouping for any lo, so a system's
+// sums do not depend on where its entries sit in the list.
+__device__ __forceinline__ double ordered_sum(const double* part, int64_t lo, int64_t hi,
+                                              int step, int off, double* red) {
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int64_t bs = blockDim.x;
+    int64_t i = lo + threadIdx.x;
+    for (; i + 7 * bs < hi; i += 8 * bs) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldcg(part + (i + k * bs) * step + off);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] += v[k];
+    }
+    for (int k = 0; i < hi; i += bs, ++k) a[k] += __ldcg(part + i * step + off);
+    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    return block_sum(s, red);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kScalarThreads)
+    bs_scalar(const SysRef* list, const int32_t* count, SysState* sys, const double* part_blk,
+              const double* part_tile) {
+    __shared__ double red[kScalarThreads / 32];
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const SysRef ref = list[i];
+        SysState& S = sys[ref.slot];
+        const int32_t ph = __ldcg(&S.phase);
+        if (ph != kSysOuter) continue;  // uniform over the CTA
+        if (KIND == kOuterNorm) {
+            const double rr = ordered_sum(part_blk, ref.blk0, ref.blk1, 1, 0, red);
+            if (threadIdx.x == 0) {
+                const double rnorm = sqrt(rr);
+                const double res = rnorm / S.bnorm;
+                S.rnorm = rnorm;
+                S.final_res = res;
+                if (res < S.tol) {
+                    S.phase = kSysDone;
+                    S.converged = 1;
+                } else if (S.outer >= S.max_outer || S.it_total >= S.max_iter) {
+                    S.phase = kSysDone;
+                    S.converged = 0;
+                } else {
+                    S.outer += 1;  // stays kSysOuter until the inner start below
+                }
+            }
+        } else {  // kStart
+            const double rz = ordered_sum(part_tile, ref.tile0, ref.tile1, 2, 0, red);
+            const double rr = ordered_sum(part_tile, ref.tile0, ref.tile1, 2, 1, red);
+            if (threadIdx.x == 0) {
+                S.rz = rz;
+                S.rr0 = rr > 0.0 ? rr : 1.0;
+                S.rr = rr;
+                S.it_inner = 0;
+                S.phase = kSysInner;
+            }
+        }
+    }
+}
+
+// ---- per-row vector steps over tiles {row0, row1, slot} ----------------------------
+
+// x += d * rnorm (the inner solution solves A d = r64 / rnorm), before the outer SpMV.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    bs_xupdate(const int4* tiles, const int32_t* count, const SysState* sys,
+               const T* __restrict__ d, double* __restrict__ x) {
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int4 tl = tiles[i];
+        if (sys_phase(sys, tl.z) != kSysOuter) continue;
+        const double s = __ldcg(&sys[tl.z].rnorm);
+        if (__ldcg(&sys[tl.z].outer) == 0) continue;  // first outer step: d is not a correction
+        for (int32_t r = tl.x + threadIdx.x; r < tl.y; r += blockDim.x)
+            x[r] = fma(double(d[r]), s, x[r]);
+    }
+}
+
+// Start an inner solve: r = r64 / rnorm, z = M^-1 r, p = z, d = 0; partials (r.z, r.r).
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    bs_inner_start(const int4* tiles, const int32_t* count, const SysState* sys,
+                   const double* __restrict__ r64, const T* __restrict__ dinv, T* __restrict__ r,
+                   T* __restrict__ z, T* __restrict__ p, T* __restrict__ d, double* part) {
+    __shared__ double red[kWarps];
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int4 tl = tiles[i];
+        T rz = T(0), rr = T(0);
+        if (sys_phase(sys, tl.z) == kSysOuter) {
+            const double rn = __ldcg(&sys[tl.z].rnorm);
+            const double sc = rn > 0.0 ? 1.0 / rn : 1.0;
+            for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x) {
+                const T ri = T(r64[row] * sc);
+                const T zi = dinv[row] * ri;
+                r[row] = ri;
+                z[row] = zi;
+                p[row] = zi;
+                d[row] = T(0);
+                rz += ri * zi;
+                rr += ri * ri;
+            }
+        }
+        const double s0 = block_sum(double(rz), red);
+        const double s1 = block_sum(double(rr), red);
+        if (threadIdx.x == 0) {
+            part[2 * int64_t(i)] = s0;
+            part[2 * int64_t(i) + 1] = s1;
+        }
+    }
+}
+
+// d += alpha p, r -= alpha Ap, z = M^-1 r; one CTA per tile writes the tile's
+// (r.z, r.r); the CTA whose tile arrives last for its system sums the system's
+// tile sums in tile order and runs the inner stopping test and beta.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    bs_update(const int4* tiles, const int32_t* count, SysState* sys, const T* __restrict__ p,
+              const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
+              T* __restrict__ z, T* __restrict__ d, double* part, unsigned int* cnt,
+              const int2* stile) {
+    __shared__ double red[kWarps];
+    __shared__ int last;
+    const int32_t i = blockIdx.x;
+    if (i >= __ldcg(count)) return;
+    const int4 tl = tiles[i];
+    const int32_t slot = tl.z;
+    const bool live = sys_phase(sys, slot) == kSysInner;
+    T rz = T(0), rr = T(0);
+    if (live) {
+        const T alpha = T(__ldcg(&sys[slot].alpha));
+        for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x) {
+            const T pi = p[row];
+            d[row] = fma(alpha, pi, d[row]);
+            const T ri = fma(-alpha, Ap[row], r[row]);
+            const T zi = dinv[row] * ri;
+            r[row] = ri;
+            z[row] = zi;
+            rz = fma(ri, zi, rz);
+            rr = fma(ri, ri, rr);
+        }
+    }
+    const double s0 = block_sum(double(rz), red);
+    const double s1 = block_sum(double(rr), red);
+    const int2 range = __ldg(stile + slot);
+    if (threadIdx.x == 0) {
+        part[2 * int64_t(i)] = s0;
+        part[2 * int64_t(i) + 1] = s1;
+        __threadfence();
+        last = atomicAdd(cnt + slot, 1u) == unsigned(range.y - range.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const double rzn = ordered_sum(part, range.x, range.y, 2, 0, red);
+    const double rrn = ordered_sum(part, range.x, range.y, 2, 1, red);
+    if (threadIdx.x == 0) {
+        cnt[slot] = 0u;
+        SysState& S = sys[slot];
+        if (!live) return;
+        S.it_inner += 1;
+        S.it_total += 1;
+        S.rr = rrn;
+        const double inner_rel = sqrt(rrn / S.rr0);
+        const double est = S.rnorm * sqrt(rrn) / S.bnorm;  // estimated |b - Ax| / |b|
+        if (!(inner_rel > S.inner_rtol) || !(est >= S.stop_frac * S.tol) ||
+            S.it_total >= S.max_iter) {
+            S.phase = kSysOuter;  // stop the inner solve; refine next step
+        } else {
+            S.beta = rzn / S.rz;
+            S.rz = rzn;
+        }
+    }
+}
+
+// p = z + beta p.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    bs_pupdate(const int4* tiles, const int32_t* count, const SysState* sys,
+               const T* __restrict__ z, T* __restrict__ p) {
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int4 tl = tiles[i];
+        if (sys_phase(sys, tl.z) != kSysInner) continue;
+        const T beta = T(__ldcg(&sys[tl.z].beta));
+        for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x)
+            p[row] = fma(beta, p[row], z[row]);
+    }
+}
+
+// ---- host side --------------------------------------------------------------------
+
+// First-fit range allocator over [0, cap).
+struct RangeAlloc {
+    std::vector<std::pair<int64_t, int64_t>> free_;  // (start, len), sorted by start
+    int64_t cap = 0, used = 0;
+    void init(int64_t c) {
+        cap = c;
+        used = 0;
+        free_.assign(1, {0, c});
+    }
+    int64_t alloc(int64_t len) {
+        for (size_t i = 0; i < free_.size(); ++i) {
+            if (free_[i].second >= len) {
+                const int64_t s = free_[i].first;
+                free_[i].first += len;
+                free_[i].second -= len;
+                if (free_[i].second == 0) free_.erase(free_.begin() + long(i));
+                used += len;
+                return s;
+            }
+        }
+        return -1;
+    }
+    void release(int64_t s, int64_t len) {
+        auto it = std::lower_bound(free_.begin(), free_.end(), std::make_pair(s, int64_t(0)));
+        it = free_.insert(it, {s, len});
+        used -= len;
+        // merge with the right, then the left neighbour
+        if (it + 1 != free_.end() && it->first + it->second == (it + 1)->first) {
+            it->second += (it + 1)->second;
+            free_.erase(it + 1);
+        }
+        if (it != free_.begin() && (it - 1)->first + (it - 1)->second == it->first) {
+            (it - 1)->second += it->second;
+            free_.erase(it);
+        }
+    }
+    int64_t largest() const {
+        int64_t m = 0;
+        for (auto& f : free_) m = std::max(m, f.second);
+        return m;
+    }
+};
+
+struct HostSys {
+    bool used = false;
+    int64_t row0 = 0, nrows_alloc = 0, z0 = 0, nnz_alloc = 0;
+    int32_t n = 0;
+    int32_t phase = kSysFree;
+    std::vector<BlockDesc> blocks;  // arena-global
+    std::vector<int4> tiles;
+};
+
+}  // namespace nm
+
+struct nm_solver {
+    int device = 0;
+    int inner = NM_F32;  // inner value precision: NM_F64 (plain PCG), NM_F32 or NM_BF16
+    int precond = 1;
+    double inner_rtol = 1e-4;
+    int max_outer = 30;
+    int64_t cap_rows = 0, cap_nnz = 0;
+    int32_t cap_sys = 0;
+    nm::RangeAlloc rows, nnz;
+    std::vector<nm::HostSys> sys;
+    // arena (device)
+    int32_t* rp = nullptr;     // [cap_rows + 16]
+    int32_t* col = nullptr;    // [cap_nnz + 16]
+    double* v64 = nullptr;     // [cap_nnz + 16]
+    void* vin = nullptr;       // inner values [cap_nnz + 16] (float / bf16 / unused for FP64)
+    double *b = nullptr, *x = nullptr, *r64 = nullptr;  // [cap_rows + 16]
+    void *p = nullptr, *Ap = nullptr, *r = nullptr, *z = nullptr, *d = nullptr, *dinv = nullptr;
+    nm::SysState* st = nullptr;     // [cap_sys]
+    nm::SysState* h_st = nullptr;   // pinned copy
+    // lists (device) and their pinned staging
+    nm::ListHdr* hdr = nullptr;
+    nm::ListHdr* h_hdr = nullptr;
+    nm::BlockDesc *iblk = nullptr, *oblk = nullptr;
+    int4 *itile = nullptr, *otile = nullptr;
+    nm::SysRef *isys = nullptr, *osys = nullptr;
+    int64_t cap_blk = 0, cap_tile = 0;
+    double *part_blk = nullptr, *part_tile = nullptr;
+    unsigned int *cnt_blk = nullptr, *cnt_tile = nullptr;  // per slot arrival counters
+    int2 *sblk = nullptr, *stile = nullptr;                // per slot ranges in the inner lists
+    int2 *h_sblk = nullptr, *h_stile = nullptr;
+    nm::BlockDesc* h_blk = nullptr;  // pinned staging (iblk then oblk)
+    int4* h_tile = nullptr;
+    nm::SysRef* h_ref = nullptr;
+    bool lists_dirty = true;
+    // CUDA graph of one chunk of inner iterations; valid while the lists (and
+    // so every kernel argument) are unchanged
+    cudaGraphExec_t chunk_exec = nullptr;
+    int32_t chunk_iters = 0;
+    bool chunk_valid = false;
+    int grid_spmv_inner = 0, grid_spmv_outer = 0, grid_vec = 0, grid_scalar = 0;
+    // pinned staging of admission uploads: a bump allocator, reset once the
+    // stream has caught up (after each step's synchronisation)
+    unsigned char* stage = nullptr;
+    size_t stage_cap = 0, stage_used = 0;
+    unsigned int* err = nullptr;
+    cudaStream_t stream = nullptr;
+    nm_solver_counters ctr{};
+    ~nm_solver();
+};
+
+nm_solver::~nm_solver() {
+    cudaFree(rp); cudaFree(col); cudaFree(v64); cudaFree(vin);
+    cudaFree(b); cudaFree(x); cudaFree(r64);
+    cudaFree(p); cudaFree(Ap); cudaFree(r); cudaFree(z); cudaFree(d); cudaFree(dinv);
+    cudaFree(st); cudaFreeHost(h_st);
+    cudaFree(hdr); cudaFreeHost(h_hdr);
+    cudaFree(iblk); cudaFree(oblk); cudaFree(itile); cudaFree(otile); cudaFree(isys); cudaFree(osys);
+    cudaFree(part_blk); cudaFree(part_tile);
+    cudaFree(cnt_blk); cudaFree(cnt_tile); cudaFree(sblk); cudaFree(stile);
+    cudaFreeHost(h_sblk); cudaFreeHost(h_stile);
+    cudaFreeHost(h_blk); cudaFreeHost(h_tile); cudaFreeHost(h_ref); cudaFreeHost(stage);
+    if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+namespace nm {
+namespace {
+
+size_t inner_bytes(int inner) { return inner == NM_F64 ? 8 : 4; }
+size_t inner_val_bytes(int inner) { return inner == NM_F64 ? 8 : (inner == NM_F32 ? 4 : 2); }
+
+int grow_lists(nm_solver* S, int64_t need_blk, int64_t need_tile) {
+    if (need_blk > S->cap_blk) {
+        const int64_t c = std::max<int64_t>(need_blk, 2 * S->cap_blk);
+        cudaFree(S->iblk); cudaFree(S->oblk); cudaFree(S->part_blk); cudaFreeHost(S->h_blk);
+        S->iblk = S->oblk = nullptr; S->part_blk = nullptr; S->h_blk = nullptr;
+        NM_CUDA_TRY(cudaMalloc(&S->iblk, sizeof(BlockDesc) * size_t(c)));
+        NM_CUDA_TRY(cudaMalloc(&S->oblk, sizeof(BlockDesc) * size_t(c)));
+        NM_CUDA_TRY(cudaMalloc(&S->part_blk, sizeof(double) * size_t(c)));
+        NM_CUDA_TRY(cudaMallocHost(&S->h_blk, sizeof(BlockDesc) * size_t(c) * 2));
+        S->cap_blk = c;
+    }
+    if (need_tile > S->cap_tile) {
+        const int64_t c = std::max<int64_t>(need_tile, 2 * S->cap_tile);
+        cudaFree(S->itile); cudaFree(S->otile); cudaFree(S->part_tile); cudaFreeHost(S->h_tile);
+        S->itile = S->otile = nullptr; S->part_tile = nullptr; S->h_tile = nullptr;
+        NM_CUDA_TRY(cudaMalloc(&S->itile, sizeof(int4) * size_t(c)));
+        NM_CUDA_TRY(cudaMalloc(&S->otile, sizeof(int4) * size_t(c)));
+        NM_CUDA_TRY(cudaMalloc(&S->part_tile, sizeof(double) * size_t(c) * 2));
+        NM_CUDA_TRY(cudaMallocHost(&S->h_tile, sizeof(int4) * size_t(c) * 2));
+        S->cap_tile = c;
+    }
+    return NM_OK;
+}
+
+// Rebuild the inner list (systems in an inner or outer phase) and the outer
+// list (systems with a pending outer step) and upload them.
+int upload_lists(nm_solver* S) {
+    int64_t nb_i = 0, nt_i = 0, nb_o = 0, nt_o = 0;
+    for (auto& h : S->sys) {
+        if (!h.used) continue;
+        if (h.phase == kSysInner || h.phase == kSysOuter) {
+            nb_i += int64_t(h.blocks.size());
+            nt_i += int64_t(h.tiles.size());
+        }
+        if (h.phase == kSysOuter) {
+            nb_o += int64_t(h.blocks.size());
+            nt_o += int64_t(h.tiles.size());
+        }
+    }
+    int st = grow_lists(S, std::max<int64_t>(1, std::max(nb_i, nb_o)),
+                        std::max<int64_t>(1, std::max(nt_i, nt_o)));
+    if (st != NM_OK) return st;
+    BlockDesc* bi = S->h_blk;
+    BlockDesc* bo = S->h_blk + S->cap_blk;
+    int4* ti = S->h_tile;
+    int4* to = S->h_tile + S->cap_tile;
+    SysRef* ri = S->h_ref;
+    SysRef* ro = S->h_ref + S->cap_sys;
+    int32_t cb_i = 0, ct_i = 0, cs_i = 0, cb_o = 0, ct_o = 0, cs_o = 0;
+    for (int32_t slot = 0; slot < S->cap_sys; ++slot) {
+        HostSys& h = S->sys[slot];
+        if (!h.used || (h.phase != kSysInner && h.phase != kSysOuter)) continue;
+        SysRef a{slot, cb_i, cb_i + int32_t(h.blocks.size()), ct_i,
+                 ct_i + int32_t(h.tiles.size()), {0, 0, 0}};
+        std::memcpy(bi + cb_i, h.blocks.data(), sizeof(BlockDesc) * h.blocks.size());
+        std::memcpy(ti + ct_i, h.tiles.data(), sizeof(int4) * h.tiles.size());
+        S->h_sblk[slot] = make_int2(a.blk0, a.blk1);
+        S->h_stile[slot] = make_int2(a.tile0, a.tile1);
+        cb_i = a.blk1;
+        ct_i = a.tile1;
+        ri[cs_i++] = a;
+        if (h.phase == kSysOuter) {
+            SysRef o{slot, cb_o, cb_o + int32_t(h.blocks.size()), ct_o,
+                     ct_o + int32_t(h.tiles.size()), {0, 0, 0}};
+            std::memcpy(bo + cb_o, h.blocks.data(), sizeof(BlockDesc) * h.blocks.size());
+            std::memcpy(to + ct_o, h.tiles.data(), sizeof(int4) * h.tiles.size());
+            cb_o = o.blk1;
+            ct_o = o.tile1;
+            ro[cs_o++] = o;
+        }
+    }
+    cudaStream_t s = S->stream;
+    *S->h_hdr = ListHdr{cb_i, ct_i, cs_i, cb_o, ct_o, cs_o, {0, 0}};
+    NM_CUDA_TRY(cudaMemcpyAsync(S->hdr, S->h_hdr, sizeof(ListHdr), cudaMemcpyHostToDevice, s));
+    if (cb_i) NM_CUDA_TRY(cudaMemcpyAsync(S->iblk, bi, sizeof(BlockDesc) * cb_i, cudaMemcpyHostToDevice, s));
+    if (cb_o) NM_CUDA_TRY(cudaMemcpyAsync(S->oblk, bo, sizeof(BlockDesc) * cb_o, cudaMemcpyHostToDevice, s));
+    if (ct_i) NM_CUDA_TRY(cudaMemcpyAsync(S->itile, ti, sizeof(int4) * ct_i, cudaMemcpyHostToDevice, s));
+    if (ct_o) NM_CUDA_TRY(cudaMemcpyAsync(S->otile, to, sizeof(int4) * ct_o, cudaMemcpyHostToDevice, s));
+    if (cs_i) NM_CUDA_TRY(cudaMemcpyAsync(S->isys, ri, sizeof(SysRef) * cs_i, cudaMemcpyHostToDevice, s));
+    if (cs_o) NM_CUDA_TRY(cudaMemcpyAsync(S->osys, ro, sizeof(SysRef) * cs_o, cudaMemcpyHostToDevice, s));
+    NM_CUDA_TRY(cudaMemcpyAsync(S->sblk, S->h_sblk, sizeof(int2) * size_t(S->cap_sys),
+                                cudaMemcpyHostToDevice, s));
+    NM_CUDA_TRY(cudaMemcpyAsync(S->stile, S->h_stile, sizeof(int2) * size_t(S->cap_sys),
+                                cudaMemcpyHostToDevice, s));
+    S->lists_dirty = false;
+    S->chunk_valid = false;
+    return NM_OK;
+}
+
+// `bytes` of pinned staging for an asynchronous upload on S->stream.  When
+// the staging buffer is full the stream is drained first (its earlier uploads
+// are then complete) and the buffer reused or grown.
+int stage_alloc(nm_solver* S, size_t bytes, void** out) {
+    bytes = (bytes + 255) & ~size_t(255);
+    if (S->stage_used + bytes > S->stage_cap) {
+        NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+        S->stage_used = 0;
+        if (bytes > S->stage_cap) {
+            cudaFreeHost(S->stage);
+            S->stage = nullptr;
+            const size_t cap = std::max<size_t>(bytes, std::max<size_t>(64u << 20, 2 * S->stage_cap));
+            NM_CUDA_TRY(cudaMallocHost(&S->stage, cap));
+            S->stage_cap = cap;
+        }
+    }
+    *out = S->stage + S->stage_used;
+    S->stage_used += bytes;
+    return NM_OK;
+}
+
+template <typename V>
+CsrView<V> arena_view(const nm_solver* S, const void* values, const BlockDesc* list,
+                      const int32_t* count) {
+    CsrView<V> M;
+    M.row_ptr = S->rp;
+    M.col_idx = S->col;
+    M.values = static_cast<const V*>(values);
+    M.desc = list;
+    M.nblk = 0;
+    M.nrows = int32_t(S->cap_rows);
+    M.short_max = kDefaultShortMax;
+    M.stage_x = 1;
+    M.nblk_dev = count;
+    return M;
+}
+
+// Grid of a persistent kernel over `count` items (at least one CTA).
+int fit_grid(int cap, int64_t count) {
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(cap, count)));
+}
+
+template <typename V, typename T>
+int launch_inner_iters(nm_solver* S, int iters) {
+    cudaStream_t s = S->stream;
+    const ListHdr* H = S->hdr;
+    const ListHdr& h = *S->h_hdr;
+    const int g_spmv = fit_grid(S->grid_spmv_inner, h.iblk);
+    const int g_vec = fit_grid(INT32_MAX, h.itile);  // one CTA per tile
+    const CsrView<V> M = arena_view<V>(S, S->vin ? S->vin : S->v64, S->iblk, &H->iblk);
+    constexpr size_t smem = spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>();
+    T* p = static_cast<T*>(S->p);
+    T* Ap = static_cast<T*>(S->Ap);
+    T* r = static_cast<T*>(S->r);
+    T* z = static_cast<T*>(S->z);
+    T* d = static_cast<T*>(S->d);
+    const T* dinv = static_cast<const T*>(S->dinv);
+    for (int it = 0; it < iters; ++it) {
+        bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
+                                                              S->cnt_blk, S->sblk, S->err);
+        bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, p, Ap, dinv, r, z, d,
+                                                S->part_tile, S->cnt_tile, S->stile);
+        bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, z, p);
+    }
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+template <typename T>
+int launch_outer(nm_solver* S) {
+    cudaStream_t s = S->stream;
+    const ListHdr* H = S->hdr;
+    const ListHdr& h = *S->h_hdr;
+    const int g_spmv = fit_grid(S->grid_spmv_outer, h.oblk);
+    const int g_vec = fit_grid(INT32_MAX, h.otile);  // one CTA per tile
+    const int g_sys = fit_grid(S->grid_scalar, h.osys);
+    const CsrView<double> M = arena_view<double>(S, S->v64, S->oblk, &H->oblk);
+    constexpr size_t smem = spmv_smem_bytes<double, double, double, kSolverTile, kSolverStages>();
+    bs_xupdate<T><<<g_vec, kThreads, 0, s>>>(S->otile, &H->otile, S->st,
+                                             static_cast<const T*>(S->d), S->x);
+    bs_spmv_outer<<<g_spmv, kCtaThreads, smem, s>>>(M, S->x, S->b, S->r64, S->st, S->part_blk,
+                                                    S->err);
+    bs_scalar<kOuterNorm><<<g_sys, kScalarThreads, 0, s>>>(S->osys, &H->osys, S->st,
+                                                           S->part_blk, S->part_tile);
+    bs_inner_start<T><<<g_vec, kThreads, 0, s>>>(
+        S->otile, &H->otile, S->st, S->r64, static_cast<const T*>(S->dinv),
+        static_cast<T*>(S->r), static_cast<T*>(S->z), static_cast<T*>(S->p),
+        static_cast<T*>(S->d), S->part_tile);
+    bs_scalar<kStart><<<g_sys, kScalarThreads, 0, s>>>(S->osys, &H->osys, S->st, S->part_blk,
+                                                       S->part_tile);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+template <typename V, typename T>
+int prepare_solver_kernels(nm_solver* S) {
+    int occ = 0;
+    // Load every kernel of a chunk now (lazy module loading), not during capture.
+    cudaFuncAttributes fa;
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_update<T>));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pupdate<T>));
+    int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
+                            spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
+    if (st != NM_OK) return st;
+    S->grid_spmv_inner = sm_count() * occ;
+    st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_outer), kCtaThreads,
+                        spmv_smem_bytes<double, double, double, kSolverTile, kSolverStages>(),
+                        &occ);
+    if (st != NM_OK) return st;
+    S->grid_spmv_outer = sm_count() * occ;
+    S->grid_vec = sm_count() * 4;
+    S->grid_scalar = sm_count() * 2;
+    return NM_OK;
+}
+
+void to_bf16(const double* v, size_t n, uint16_t* out) {
+    for (size_t i = 0; i < n; ++i) {
+        const float f = static_cast<float>(v[i]);
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        if ((u & 0x7fffffffu) > 0x7f800000u) {
+            out[i] = static_cast<uint16_t>((u >> 16) | 0x40u);  // quiet NaN
+        } else {
+            u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even
+            out[i] = static_cast<uint16_t>(u >> 16);
+        }
+    }
+}
+
+}  // namespace
+}  // namespace nm
+
+using nm::fail;
+
+extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_systems,
+                                const nm_solver_opts* opts, nm_solver** out) {
+    using namespace nm;
+    clear_error();
+    if (!out) return fail(NM_ERR_INVALID, "nm_solver_create: out is NULL");
+    *out = nullptr;
+    if (max_rows <= 0 || max_nnz <= 0 || max_systems <= 0)
+        return fail(NM_ERR_INVALID, "nm_solver_create: capacities must be positive");
+    if (max_rows > INT32_MAX - 4096 || max_nnz > INT32_MAX - 4096)
+        return fail(NM_ERR_INVALID, "nm_solver_create: capacities exceed the int32 index range");
+    auto S = std::make_unique<nm_solver>();
+    if (opts) {
+        S->inner = opts->inner;
+        S->precond = opts->precond;
+        if (opts->inner_rtol > 0) S->inner_rtol = opts->inner_rtol;
+        if (opts->max_outer > 0) S->max_outer = opts->max_outer;
+    }
+    if (S->inner != NM_F64 && S->inner != NM_F32 && S->inner != NM_BF16)
+        return fail(NM_ERR_TYPE, "nm_solver_create: unknown inner precision %d", S->inner);
+    NM_CUDA_TRY(cudaGetDevice(&S->device));
+    S->cap_rows = max_rows;
+    S->cap_nnz = max_nnz;
+    S->cap_sys = max_systems;
+    S->rows.init(max_rows);
+    S->nnz.init(max_nnz);
+    S->sys.resize(size_t(max_systems));
+    const size_t R = size_t(max_rows) + 16, Z = size_t(max_nnz) + 16;
+    const size_t tb = inner_bytes(S->inner);
+    NM_CUDA_TRY(cudaMalloc(&S->rp, sizeof(int32_t) * R));
+    NM_CUDA_TRY(cudaMemset(S->rp, 0, sizeof(int32_t) * R));
+    NM_CUDA_TRY(cudaMalloc(&S->col, sizeof(int32_t) * Z));
+    NM_CUDA_TRY(cudaMemset(S->col, 0, sizeof(int32_t) * Z));
+    NM_CUDA_TRY(cudaMalloc(&S->v64, sizeof(double) * Z));
+    if (S->inner != NM_F64) NM_CUDA_TRY(cudaMalloc(&S->vin, inner_val_bytes(S->inner) * Z));
+    NM_CUDA_TRY(cudaMalloc(&S->b, sizeof(double) * R));
+    NM_CUDA_TRY(cudaMalloc(&S->x, sizeof(double) * R));
+    NM_CUDA_TRY(cudaMalloc(&S->r64, sizeof(double) * R));
+    for (void** v : {&S->p, &S->Ap, &S->r, &S->z, &S->d, &S->dinv}) {
+        NM_CUDA_TRY(cudaMalloc(v, tb * R));
+        NM_CUDA_TRY(cudaMemset(*v, 0, tb * R));
+    }
+    NM_CUDA_TRY(cudaMalloc(&S->st, sizeof(SysState) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMemset(S->st, 0, sizeof(SysState) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_st, sizeof(SysState) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMalloc(&S->hdr, sizeof(ListHdr)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_hdr, sizeof(ListHdr)));
+    NM_CUDA_TRY(cudaMalloc(&S->isys, sizeof(SysRef) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMalloc(&S->osys, sizeof(SysRef) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 2));
+    for (unsigned int** c : {&S->cnt_blk, &S->cnt_tile}) {
+        NM_CUDA_TRY(cudaMalloc(c, sizeof(unsigned int) * size_t(max_systems)));
+        NM_CUDA_TRY(cudaMemset(*c, 0, sizeof(unsigned int) * size_t(max_systems)));
+    }
+    for (int2** r : {&S->sblk, &S->stile}) {
+        NM_CUDA_TRY(cudaMalloc(r, sizeof(int2) * size_t(max_systems)));
+        NM_CUDA_TRY(cudaMemset(*r, 0, sizeof(int2) * size_t(max_systems)));
+    }
+    NM_CUDA_TRY(cudaMallocHost(&S->h_sblk, sizeof(int2) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_stile, sizeof(int2) * size_t(max_systems)));
+    int st = grow_lists(S.get(), 1024, 1024);
+    if (st != NM_OK) return st;
+    NM_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    S->err = device_error_word();
+    if (!S->err) return fail(NM_ERR_CUDA, "nm_solver_create: cannot map the device error word");
+    switch (S->inner) {
+        case NM_F64: st = prepare_solver_kernels<double, double>(S.get()); break;
+        case NM_F32: st = prepare_solver_kernels<float, float>(S.get()); break;
+        default: st = prepare_solver_kernels<__nv_bfloat16, float>(S.get()); break;
+    }
+    if (st != NM_OK) return st;
+    *out = S.release();
+    return NM_OK;
+}
+
+extern "C" int nm_solver_destroy(nm_solver* S) {
+    nm::clear_error();
+    if (S) cudaStreamSynchronize(S->stream);
+    delete S;
+    return NM_OK;
+}
+
+namespace nm {
+namespace {
+
+// Runs f(begin, end) over [0, n) on up to hardware_concurrency threads, in
+// chunks of at least `grain` items.
+template <class F>
+void parallel_for(int64_t n, int64_t grain, const F& f) {
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / std::max<int64_t>(1, grain)));
+    if (nt <= 1) {
+        if (n > 0) f(int64_t(0), n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(size_t(nt));
+    for (int64_t t = 0; t < nt; ++t)
+        th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt); });
+    for (auto& x : th) x.join();
+}
+
+// One admission: inputs, the ranges it was given, its pinned staging.
+struct AdmitJob {
+    const int32_t* row_ptr;
+    const int32_t* col_idx;
+    const double* values;
+    int32_t n;
+    const double* b;
+    const double* x0;
+    double tol;
+    int32_t max_iter;
+    // assigned
+    int32_t slot = -1;
+    int64_t r0 = 0, nrows_alloc = 0, z0 = 0, nnz_alloc = 0;
+    unsigned char* stage = nullptr;
+    int bad_col = -1;     // an invalid column index found by the preparation
+    bool bad_rp = false;  // row_ptr decreases somewhere
+    std::vector<BlockDesc> blocks;
+    std::vector<int4> tiles;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Staging layout of a job: row_ptr, col_idx, FP64 values, inner values, b,
+// x0, inverse diagonal, SysState.
+void stage_sizes(const nm_solver* S, const AdmitJob& J, size_t sz[8]) {
+    const size_t n = size_t(J.n), nz = size_t(J.row_ptr[J.n]);
+    sz[0] = align256(sizeof(int32_t) * (n + 1));
+    sz[1] = align256(sizeof(int32_t) * nz);
+    sz[2] = align256(sizeof(double) * nz);
+    sz[3] = align256(S->inner != NM_F64 ? inner_val_bytes(S->inner) * nz : 0);
+    sz[4] = align256(sizeof(double) * n);
+    sz[5] = align256(J.x0 ? sizeof(double) * n : 0);
+    sz[6] = align256(inner_bytes(S->inner) * n);
+    sz[7] = align256(sizeof(SysState));
+}
+
+size_t stage_total(const nm_solver* S, const AdmitJob& J) {
+    size_t sz[8];
+    stage_sizes(S, J, sz);
+    size_t t = 0;
+    for (size_t q : sz) t += q;
+    return t;
+}
+
+// Cheap checks before any allocation.
+int job_check(const AdmitJob& J) {
+    if (!J.row_ptr || !J.b) return fail(NM_ERR_INVALID, "nm_solver_admit: NULL argument");
+    if (J.n <= 0) return fail(NM_ERR_INVALID, "nm_solver_admit: non-positive dimensions");
+    if (J.row_ptr[0] != 0) return fail(NM_ERR_INVALID, "nm_solver_admit: row_ptr[0] must be 0");
+    if (J.row_ptr[J.n] < 0) return fail(NM_ERR_INVALID, "nm_solver_admit: row_ptr decreases");
+    if (J.row_ptr[J.n] > 0 && (!J.col_idx || !J.values))
+        return fail(NM_ERR_INVALID, "nm_solver_admit: NULL array");
+    return NM_OK;
+}
+
+// Slot and arena ranges; NM_ERR_NOMEM when they do not fit.
+int job_alloc(nm_solver* S, AdmitJob& J) {
+    int32_t slot = -1;
+    for (int32_t k = 0; k < S->cap_sys; ++k)
+        if (!S->sys[k].used) {
+            slot = k;
+            break;
+        }
+    if (slot < 0) return fail(NM_ERR_NOMEM, "nm_solver_admit: all %d system slots are in use", S->cap_sys);
+    const int32_t nz = J.row_ptr[J.n];
+    // One spare row for the closing row_ptr entry; nonzero ranges padded to 8.
+    const int64_t nrows_alloc = ((int64_t(J.n) + 1 + 3) / 4) * 4;
+    const int64_t nnz_alloc = ((int64_t(nz) + 7) / 8) * 8 + 8;
+    const int64_t r0 = S->rows.alloc(nrows_alloc);
+    if (r0 < 0) return fail(NM_ERR_NOMEM, "nm_solver_admit: no room for %d rows", J.n);
+    const int64_t z0 = S->nnz.alloc(nnz_alloc);
+    if (z0 < 0) {
+        S->rows.release(r0, nrows_alloc);
+        return fail(NM_ERR_NOMEM, "nm_solver_admit: no room for %d nonzeros", nz);
+    }
+    S->sys[slot].used = true;  // reserved; filled in by job_commit
+    J.slot = slot;
+    J.r0 = r0;
+    J.nrows_alloc = nrows_alloc;
+    J.z0 = z0;
+    J.nnz_alloc = nnz_alloc;
+    return NM_OK;
+}
+
+void job_release(nm_solver* S, AdmitJob& J) {
+    if (J.slot < 0) return;
+    S->rows.release(J.r0, J.nrows_alloc);
+    S->nnz.release(J.z0, J.nnz_alloc);
+    S->sys[J.slot] = HostSys{};
+    J.slot = -1;
+}
+
+// Host preparation of one job into its staging; touches nothing shared, so
+// jobs run concurrently.  `inner_threads`: parallelise this job's rows.
+void job_prep(const nm_solver* S, AdmitJob& J, bool inner_threads) {
+    size_t sz[8];
+    stage_sizes(S, J, sz);
+    unsigned char* q = J.stage;
+    int32_t* grp = reinterpret_cast<int32_t*>(q); q += sz[0];
+    int32_t* gci = reinterpret_cast<int32_t*>(q); q += sz[1];
+    double* v64s = reinterpret_cast<double*>(q); q += sz[2];
+    void* vins = q; q += sz[3];
+    double* bs = reinterpret_cast<double*>(q); q += sz[4];
+    double* x0s = reinterpret_cast<double*>(q); q += sz[5];
+    void* dinvs = q; q += sz[6];
+    SysState* ss = reinterpret_cast<SysState*>(q);
+    const int32_t n = J.n;
+    const int32_t* rp = J.row_ptr;
+    const int32_t* ci = J.col_idx;
+    const double* val = J.values;
+    const int32_t r0 = int32_t(J.r0), z0 = int32_t(J.z0);
+    const bool dbl = inner_bytes(S->inner) == 8;
+    const int precond = S->precond;
+    const int inner = S->inner;
+    for (int32_t i = 0; i < n; ++i)
+        if (rp[i + 1] < rp[i]) {
+            J.bad_rp = true;
+            return;
+        }
+    std::mutex mu;
+    auto rows = [&](int64_t i0, int64_t i1) {
+        int badc = -1;
+        for (int64_t i = i0; i < i1; ++i) {
+            grp[i] = z0 + rp[i];
+            double dg = 0.0;
+            for (int32_t j = rp[i]; j < rp[i + 1]; ++j) {
+                const int32_t c = ci[j];
+                if ((c < 0 || c >= n) && badc < 0) badc = c;
+                gci[j] = r0 + c;
+                v64s[j] = val[j];
+                if (inner == NM_F32) static_cast<float*>(vins)[j] = static_cast<float>(val[j]);
+                if (c == i) dg += val[j];
+            }
+            const double di = (precond && dg != 0.0) ? 1.0 / dg : 1.0;
+            if (dbl) static_cast<double*>(dinvs)[i] = di;
+            else static_cast<float*>(dinvs)[i] = float(di);
+            bs[i] = J.b[i];
+            if (J.x0) x0s[i] = J.x0[i];
+        }
+        if (inner == NM_BF16 && i1 > i0)
+            to_bf16(val + rp[i0], size_t(rp[i1] - rp[i0]), static_cast<uint16_t*>(vins) + rp[i0]);
+        std::lock_guard<std::mutex> g(mu);
+        if (badc >= 0 && J.bad_col < 0) J.bad_col = badc;
+    };
+    if (inner_threads) parallel_for(n, 65536, rows);
+    else rows(0, n);
+    grp[n] = z0 + rp[n];
+    if (J.bad_col >= 0) return;
+    // |b|^2 in row order (the same bits however the rows were prepared)
+    double bb = 0.0;
+    for (int32_t i = 0; i < n; ++i) bb += J.b[i] * J.b[i];
+    // row blocks (default partition), arena-global descriptors and x windows
+    std::vector<int32_t> blk;
+    build_row_blocks(rp, n, kSolverTile, kDefaultMaxRows, kDefaultShortMax, blk, nullptr);
+    const int64_t nb = int64_t(blk.size()) - 1;
+    J.blocks.assign(size_t(nb), BlockDesc{});
+    const int32_t cap_rows = int32_t(S->cap_rows);
+    const int32_t slot = J.slot;
+    auto blocks = [&](int64_t k0, int64_t k1) {
+        std::vector<int32_t> scratch;
+        for (int64_t k = k0; k < k1; ++k) {
+            BlockDesc& dsc = J.blocks[size_t(k)];
+            const int32_t lz0 = rp[blk[k]], lz1 = rp[blk[k + 1]];
+            int32_t nlong = 0;
+            for (int32_t rr = blk[k]; rr < blk[k + 1]; ++rr)
+                nlong += (rp[rr + 1] - rp[rr]) > kDefaultShortMax;
+            dsc.rz = make_int4(r0 + blk[k], r0 + blk[k + 1], z0 + lz0, z0 + lz1);
+            dsc.aux = make_int4(nlong, slot, 0, 0);
+            if (lz1 - lz0 > kSolverTile) {
+                dsc.xs = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
+                dsc.xl = make_int4(0, 0, 0, 0);
+            } else {
+                block_xwindows(gci, lz0, lz1, cap_rows, xwin_capacity(kSolverTile), scratch,
+                               &dsc.xs, &dsc.xl);
+            }
+        }
+    };
+    if (inner_threads) parallel_for(nb, 64, blocks);
+    else blocks(0, nb);
+    J.tiles.clear();
+    for (int32_t t0 = 0; t0 < n; t0 += kTileRows)
+        J.tiles.push_back(make_int4(r0 + t0, r0 + std::min(n, t0 + kTileRows), slot, 0));
+    std::memset(ss, 0, sizeof(SysState));
+    ss->row0 = r0;
+    ss->n = n;
+    ss->max_iter = J.max_iter;
+    ss->max_outer = S->max_outer;
+    ss->tol = J.tol;
+    ss->bnorm = bb > 0.0 ? std::sqrt(bb) : 1.0;
+    ss->inner_rtol = S->inner == NM_F64 ? 0.0 : S->inner_rtol;
+    ss->stop_frac = S->inner == NM_F64 ? 1.0 : 0.5;
+    ss->phase = kSysOuter;
+}
+
+// Asynchronous uploads of a prepared job and its host record.
+int job_commit(nm_solver* S, AdmitJob& J) {
+    size_t sz[8];
+    stage_sizes(S, J, sz);
+    unsigned char* q = J.stage;
+    unsigned char* ptr[8];
+    for (int k = 0; k < 8; ++k) {
+        ptr[k] = q;
+        q += sz[k];
+    }
+    const size_t n = size_t(J.n), nz = size_t(J.row_ptr[J.n]);
+    const size_t tb = inner_bytes(S->inner), vb = inner_val_bytes(S->inner);
+    cudaStream_t s = S->stream;
+    const int64_t r0 = J.r0, z0 = J.z0;
+    NM_CUDA_TRY(cudaMemcpyAsync(S->rp + r0, ptr[0], sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s));
+    if (nz) {
+        NM_CUDA_TRY(cudaMemcpyAsync(S->col + z0, ptr[1], sizeof(int32_t) * nz, cudaMemcpyHostToDevice, s));
+        NM_CUDA_TRY(cudaMemcpyAsync(S->v64 + z0, ptr[2], sizeof(double) * nz, cudaMemcpyHostToDevice, s));
+        if (S->inner != NM_F64)
+            NM_CUDA_TRY(cudaMemcpyAsync(static_cast<unsigned char*>(S->vin) + vb * size_t(z0), ptr[3],
+                                        vb * nz, cudaMemcpyHostToDevice, s));
+    }
+    NM_CUDA_TRY(cudaMemcpyAsync(S->b + r0, ptr[4], sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if (J.x0) {
+        NM_CUDA_TRY(cudaMemcpyAsync(S->x + r0, ptr[5], sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    } else {
+        NM_CUDA_TRY(cudaMemsetAsync(S->x + r0, 0, sizeof(double) * n, s));
+    }
+    NM_CUDA_TRY(cudaMemsetAsync(static_cast<unsigned char*>(S->d) + tb * size_t(r0), 0, tb * n, s));
+    NM_CUDA_TRY(cudaMemcpyAsync(static_cast<unsigned char*>(S->dinv) + tb * size_t(r0), ptr[6], tb * n,
+                                cudaMemcpyHostToDevice, s));
+    const SysState* ss = reinterpret_cast<const SysState*>(ptr[7]);
+    S->h_st[J.slot] = *ss;
+    NM_CUDA_TRY(cudaMemcpyAsync(S->st + J.slot, ss, sizeof(SysState), cudaMemcpyHostToDevice, s));
+    HostSys& h = S->sys[J.slot];
+    h.used = true;
+    h.row0 = J.r0;
+    h.nrows_alloc = J.nrows_alloc;
+    h.z0 = J.z0;
+    h.nnz_alloc = J.nnz_alloc;
+    h.n = J.n;
+    h.phase = kSysOuter;
+    h.blocks = std::move(J.blocks);
+    h.tiles = std::move(J.tiles);
+    S->lists_dirty = true;
+    return NM_OK;
+}
+
+// Admits jobs[0..count) in order, preparing them in parallel; stops at the
+// first one that does not fit.  *admitted = jobs admitted.
+int admit_jobs(nm_solver* S, AdmitJob* jobs, int32_t count, int32_t* admitted) {
+    *admitted = 0;
+    int32_t done = 0;
+    // Sub-batches bounded by a staging budget so pinned staging stays modest.
+    constexpr size_t kBatchStage = size_t(512) << 20;
+    while (done < count) {
+        int32_t k = done;
+        size_t bytes = 0;
+        int st = NM_OK;
+        for (; k < count; ++k) {
+            st = job_check(jobs[k]);
+            if (st != NM_OK) break;
+            const size_t tb = stage_total(S, jobs[k]);
+            if (k > done && bytes + tb > kBatchStage) break;
+            st = job_alloc(S, jobs[k]);
+            if (st != NM_OK) break;
+            bytes += tb;
+        }
+        const int32_t end = k;
+        if (end == done) return st;  // the first job of this sub-batch was refused
+        unsigned char* base = nullptr;
+        int sst = stage_alloc(S, bytes, reinterpret_cast<void**>(&base));
+        if (sst != NM_OK) {
+            for (int32_t j = done; j < end; ++j) job_release(S, jobs[j]);
+            return sst;
+        }
+        for (int32_t j = done; j < end; ++j) {
+            jobs[j].stage = base;
+            base += stage_total(S, jobs[j]);
+        }
+        const bool one = end - done == 1;
+        if (one) {
+            job_prep(S, jobs[done], true);
+        } else {
+            parallel_for(end - done, 1, [&](int64_t a, int64_t b) {
+                for (int64_t j = a; j < b; ++j) job_prep(S, jobs[done + j], false);
+            });
+        }
+        for (int32_t j = done; j < end; ++j) {
+            if (jobs[j].bad_col >= 0 || jobs[j].bad_rp) {
+                const AdmitJob& b = jobs[j];
+                const int c = b.bad_col;
+                const bool rp_bad = b.bad_rp;
+                const int32_t bn = b.n;
+                for (int32_t q = j; q < end; ++q) job_release(S, jobs[q]);
+                if (rp_bad) return fail(NM_ERR_INVALID, "nm_solver_admit: row_ptr decreases");
+                return fail(NM_ERR_INVALID, "nm_solver_admit: column %d outside [0, %d)", c, bn);
+            }
+            const int cst = job_commit(S, jobs[j]);
+            if (cst != NM_OK) return cst;
+            ++*admitted;
+        }
+        done = end;
+        if (st != NM_OK) return st;  // stopped early (no room or an invalid system)
+    }
+    return NM_OK;
+}
+
+}  // namespace
+}  // namespace nm
+
+extern "C" int nm_solver_admit(nm_solver* S, const int32_t* row_ptr, const int32_t* col_idx,
+                               const double* values, int32_t n, const double* b, const double* x0,
+                               double tol, int32_t max_iter, int32_t* slot_out) {
+    using namespace nm;
+    clear_error();
+    if (!S || !slot_out) return fail(NM_ERR_INVALID, "nm_solver_admit: NULL argument");
+    AdmitJob J{row_ptr, col_idx, values, n, b, x0, tol, max_iter};
+    int32_t admitted = 0;
+    const int st = admit_jobs(S, &J, 1, &admitted);
+    if (st != NM_OK) return st;
+    *slot_out = J.slot;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t* const* row_ptr,
+                                     const int32_t* const* col_idx, const double* const* values,
+                                     const int32_t* n, const double* const* b, double tol,
+                                     int32_t max_iter, int32_t* slots, int32_t* admitted) {
+    using namespace nm;
+    clear_error();
+    if (!S || count < 0 || !slots || !admitted || (count > 0 && (!row_ptr || !n || !b)))
+        return fail(NM_ERR_INVALID, "nm_solver_admit_batch: NULL argument");
+    std::vector<AdmitJob> jobs;
+    jobs.reserve(size_t(count));
+    for (int32_t k = 0; k < count; ++k)
+        jobs.push_back(AdmitJob{row_ptr[k], col_idx ? col_idx[k] : nullptr,
+                                values ? values[k] : nullptr, n[k], b[k], nullptr, tol, max_iter});
+    const int st = admit_jobs(S, jobs.data(), count, admitted);
+    for (int32_t k = 0; k < *admitted; ++k) slots[k] = jobs[k].slot;
+    if (st == NM_ERR_NOMEM) {
+        clear_error();
+        return NM_OK;  // the rest did not fit now; *admitted tells how many did
+    }
+    return st;
+}
+
+extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
+    using namespace nm;
+    using clk = std::chrono::steady_clock;
+    clear_error();
+    if (!S) return fail(NM_ERR_INVALID, "nm_solver_step: NULL solver");
+    int st = NM_OK;
+    auto t0 = clk::now();
+    auto lap = [&t0](double& acc) {
+        const auto t = clk::now();
+        acc += std::chrono::duration<double>(t - t0).count();
+        t0 = t;
+    };
+    if (S->lists_dirty) {
+        st = upload_lists(S);
+        if (st != NM_OK) return st;
+        S->ctr.list_uploads += 1;
+    }
+    lap(S->ctr.s_lists);
+    const ListHdr& H = *S->h_hdr;
+    if (H.isys == 0) {
+        if (n_done) *n_done = 0;
+        return NM_OK;
+    }
+    S->ctr.steps += 1;
+    if (H.osys > 0) {
+        st = S->inner == NM_F64 ? launch_outer<double>(S) : launch_outer<float>(S);
+        if (st != NM_OK) return st;
+        S->ctr.outer_launches += 1;
+    }
+    lap(S->ctr.s_outer);
+    if (iters > 0) {
+        if (!S->chunk_valid || S->chunk_iters != iters) {
+            S->ctr.graph_captures += 1;
+            // (Re)capture the chunk; update the executable graph in place when
+            // only kernel arguments changed.
+            cudaGraph_t g = nullptr;
+            NM_CUDA_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+            switch (S->inner) {
+                case NM_F64: st = launch_inner_iters<double, double>(S, iters); break;
+                case NM_F32: st = launch_inner_iters<float, float>(S, iters); break;
+                default: st = launch_inner_iters<__nv_bfloat16, float>(S, iters); break;
+            }
+            const cudaError_t ec = cudaStreamEndCapture(S->stream, &g);
+            if (st != NM_OK) {
+                if (g) cudaGraphDestroy(g);
+                return st;
+            }
+            if (ec != cudaSuccess)
+                return fail(NM_ERR_CUDA, "solver chunk capture failed: %s", cudaGetErrorString(ec));
+            bool updated = false;
+            if (S->chunk_exec && S->chunk_iters == iters) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(S->chunk_exec, g, &info) == cudaSuccess;
+                cudaGetLastError();  // an update refusal is not an error
+            }
+            if (!updated) {
+                S->ctr.graph_instantiations += 1;
+                if (S->chunk_exec) cudaGraphExecDestroy(S->chunk_exec);
+                S->chunk_exec = nullptr;
+                const cudaError_t ei = cudaGraphInstantiate(&S->chunk_exec, g, 0);
+                if (ei != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    return fail(NM_ERR_CUDA, "solver chunk instantiate failed: %s",
+                                cudaGetErrorString(ei));
+                }
+            }
+            cudaGraphDestroy(g);
+            S->chunk_iters = iters;
+            S->chunk_valid = true;
+        }
+        lap(S->ctr.s_capture);
+        NM_CUDA_TRY(cudaGraphLaunch(S->chunk_exec, S->stream));
+        S->ctr.inner_iterations += iters;
+    }
+    NM_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(SysState) * size_t(S->cap_sys),
+                                cudaMemcpyDeviceToHost, S->stream));
+    NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    lap(S->ctr.s_run);
+    S->stage_used = 0;  // every staged upload has landed
+    st = nm_check_device_errors();
+    if (st != NM_OK) return st;
+    int32_t done = 0;
+    for (int32_t k = 0; k < S->cap_sys; ++k) {
+        HostSys& h = S->sys[k];
+        if (!h.used) continue;
+        const int32_t ph = S->h_st[k].phase;
+        if (ph != h.phase) {
+            // membership of the outer list changes with every phase change
+            S->lists_dirty = true;
+            if (ph == kSysDone) ++done;
+            h.phase = ph;
+        }
+    }
+    if (n_done) *n_done = done;
+    lap(S->ctr.s_scan);
+    return NM_OK;
+}
+
+extern "C" int nm_solver_counters_get(const nm_solver* S, nm_solver_counters* out) {
+    nm::clear_error();
+    if (!S || !out) return fail(NM_ERR_INVALID, "nm_solver_counters_get: NULL argument");
+    *out = S->ctr;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_status(const nm_solver* S, int32_t slot, int32_t* phase,
+                                nm_cg_result* res, int32_t* outer) {
+    using namespace nm;
+    clear_error();
+    if (!S || slot < 0 || slot >= S->cap_sys || !S->sys[slot].used)
+        return fail(NM_ERR_INVALID, "nm_solver_status: no system in slot %d", slot);
+    const SysState& ss = S->h_st[slot];
+    if (phase) *phase = S->sys[slot].phase;
+    if (res) {
+        res->iters = ss.it_total;
+        res->final_res = ss.final_res;
+        res->converged = ss.converged;
+    }
+    if (outer) *outer = ss.outer;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_take(nm_solver* S, int32_t slot, double* x_host) {
+    using namespace nm;
+    clear_error();
+    if (!S || slot < 0 || slot >= S->cap_sys || !S->sys[slot].used)
+        return fail(NM_ERR_INVALID, "nm_solver_take: no system in slot %d", slot);
+    HostSys& h = S->sys[slot];
+    if (x_host)
+        NM_CUDA_TRY(cudaMemcpyAsync(x_host, S->x + h.row0, sizeof(double) * size_t(h.n),
+                                    cudaMemcpyDeviceToHost, S->stream));
+    NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    S->rows.release(h.row0, h.nrows_alloc);
+    S->nnz.release(h.z0, h.nnz_alloc);
+    const bool was_active = h.phase == kSysInner || h.phase == kSysOuter;
+    h = HostSys{};
+    S->h_st[slot].phase = kSysFree;
+    NM_CUDA_TRY(cudaMemcpyAsync(&S->st[slot].phase, &S->h_st[slot].phase, sizeof(int32_t),
+                                cudaMemcpyHostToDevice, S->stream));
+    NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (was_active) S->lists_dirty = true;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_info(const nm_solver* S, int64_t* free_rows, int64_t* free_nnz,
+                              int32_t* active, int32_t* free_slots) {
+    using namespace nm;
+    clear_error();
+    if (!S) return fail(NM_ERR_INVALID, "nm_solver_info: NULL solver");
+    if (free_rows) *free_rows = S->rows.largest();
+    if (free_nnz) *free_nnz = S->nnz.largest();
+    int32_t a = 0, f = 0;
+    for (auto& h : S->sys) {
+        if (!h.used) ++f;
+        else if (h.phase == kSysInner || h.phase == kSysOuter) ++a;
+    }
+    if (active) *active = a;
+    if (free_slots) *free_slots = f;
+    return NM_OK;
+}

@@ -47,6 +47,35 @@ static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     }
 }
 
+template <typename V, typename X, typename A, int TILE>
+static size_t smem_stages(int stages) {
+    switch (stages) {
+        case 2: return spmv_smem_bytes<V, X, A, TILE, 2>();
+        case 3: return spmv_smem_bytes<V, X, A, TILE, 3>();
+        case 4: return spmv_smem_bytes<V, X, A, TILE, 4>();
+        default: return 0;
+    }
+}
+
+template <typename V, typename X, typename A>
+static size_t smem_tile(int tile, int stages) {
+    switch (tile) {
+        case 1024: return smem_stages<V, X, A, 1024>(stages);
+        case 2048: return smem_stages<V, X, A, 2048>(stages);
+        case 4096: return smem_stages<V, X, A, 4096>(stages);
+        default: return 0;
+    }
+}
+
+size_t spmv_smem_for(int dtype, int tile, int stages) {
+    switch (dtype) {
+        case NM_F64: return smem_tile<double, double, double>(tile, stages);
+        case NM_F32: return smem_tile<float, float, float>(tile, stages);
+        case NM_BF16: return smem_tile<__nv_bfloat16, float, float>(tile, stages);
+        default: return 0;
+    }
+}
+
 int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
     switch (A->dtype) {
         case NM_F64:

@@ -102,7 +102,28 @@ struct SpmvSmem {
     int32_t long_rows[kThreads];
     int32_t warp_cnt[kWarps];
     A red[kWarps + 1];
+    double blk_red[2][kWarps];  // per-block epilogue sums, double-buffered by block parity
 };
+
+// Per-block sum of one value per consumer thread, in a fixed order (warp
+// shuffle tree, then warps 0..7), written by consumer thread 0 to *out.  One
+// consumer barrier; the two buffers alternate with the block's parity, which
+// makes a second barrier unnecessary (a warp can only write a buffer again
+// after the barrier of the next block, which thread 0 reaches after reading).
+__device__ __forceinline__ void consumer_block_sum(double v, double (*buf)[kWarps],
+                                                   int64_t parity, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    double* b = buf[parity & 1];
+    if (lane == 0) b[warp] = v;
+    consumer_sync();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += b[w];
+        *out = s;
+    }
+}
 
 __device__ __forceinline__ BlockDesc load_desc(const BlockDesc* p) {
     const int4* q = reinterpret_cast<const int4*>(p);
@@ -114,18 +135,26 @@ __device__ __forceinline__ BlockDesc load_desc(const BlockDesc* p) {
     return d;
 }
 
+// Every block is computed.
+struct AllBlocks {
+    __device__ __forceinline__ bool operator()(const BlockDesc&) const { return true; }
+};
+
 // Producer: stage the block described by d into stage s (its nonzeros,
-// row_ptr slice and, when M.stage_x, its x windows).
+// row_ptr slice and, when M.stage_x, its x windows).  A block the gate
+// rejected (d.aux.z = 1, decided when the descriptor was loaded) is not
+// staged; it reaches the consumers marked skipped.
 template <typename V, typename X, typename A, int TILE, int STAGES>
 __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restrict__ x,
                                            BlockDesc d, SpmvSmem<V, X, A, TILE, STAGES>& sm,
                                            int s) {
     const int32_t r0 = d.rz.x, r1 = d.rz.y, z0 = d.rz.z, z1 = d.rz.w;
+    const bool skip = d.aux.z != 0;
     const bool long_row = z1 - z0 > TILE;
-    const bool stage_x = !long_row && M.stage_x && d.xs.x >= 0;
+    const bool stage_x = !skip && !long_row && M.stage_x && d.xs.x >= 0;
     if (!stage_x) d.xs.x = -1;
     sm.meta[s] = d;
-    if (long_row) {  // read from global by the consumers
+    if (skip || long_row) {  // nothing staged (long rows are read from global)
         mbar_arrive_expect_tx(&sm.full[s], 0u);
         return;
     }
@@ -269,12 +298,14 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
 // threads.  Returns false on the threads of a CTA where a bounded wait gave
 // up (the error word is set; partial results must not be used).  On return
 // no TMA copy into this CTA's shared memory is pending.
-template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
-__device__ __forceinline__ bool spmv_pipeline(const CsrView<V>& M, const X* __restrict__ x,
+template <typename V, typename X, typename A, int TILE, int STAGES, class Epi,
+          class Gate = AllBlocks>
+__device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict__ x,
                                               SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi,
-                                              unsigned int* err) {
+                                              unsigned int* err, const Gate& gate = Gate()) {
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
+    if (M.nblk_dev) M.nblk = __ldg(M.nblk_dev);
     if (t == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
@@ -293,11 +324,17 @@ __device__ __forceinline__ bool spmv_pipeline(const CsrView<V>& M, const X* __re
         bool ok = true;
         int s = 0;
         int64_t k = 0;
+        // descriptors (with the gate's verdict in aux.z) are loaded one block ahead
+        auto fetch = [&](int64_t bb) {
+            BlockDesc dd = load_desc(M.desc + bb);
+            dd.aux.z = gate(dd) ? 0 : 1;
+            return dd;
+        };
         BlockDesc next{};
-        if (int64_t(blockIdx.x) < M.nblk) next = load_desc(M.desc + blockIdx.x);
+        if (int64_t(blockIdx.x) < M.nblk) next = fetch(blockIdx.x);
         for (int64_t b = blockIdx.x; b < M.nblk; b += gridDim.x, ++k) {
             const BlockDesc d = next;
-            if (b + gridDim.x < M.nblk) next = load_desc(M.desc + b + gridDim.x);
+            if (b + gridDim.x < M.nblk) next = fetch(b + gridDim.x);
             if (k >= STAGES) {
                 if (!mbar_wait_bounded(&sm.empty[s], (empty_par >> s) & 1u)) {
                     atomicOr(err, kErrWaitTimeout);
@@ -334,10 +371,16 @@ __device__ __forceinline__ bool spmv_pipeline(const CsrView<V>& M, const X* __re
         }
         full_par ^= 1u << s;
         const BlockDesc d = ok ? sm.meta[s] : load_desc(M.desc + b);
+        // A block the producer skipped (nothing staged) runs the same barrier
+        // schedule as any other -- it depends only on d.rz and d.aux.x, equal in
+        // the staged and the global descriptor -- with data access off, so
+        // consumers that saw the stage and consumers that gave up stay in step.
+        const bool active = ok && d.aux.z == 0;
         if (d.rz.w - d.rz.z > TILE)
-            spmv_long_row<V, X, A, TILE, STAGES>(M, ok, d.rz.x, d.rz.z, d.rz.w, x, sm, epi);
+            spmv_long_row<V, X, A, TILE, STAGES>(M, active, d.rz.x, d.rz.z, d.rz.w, x, sm, epi);
         else
-            spmv_rows<V, X, A, TILE, STAGES>(M, s, ok, d, x, sm, epi);
+            spmv_rows<V, X, A, TILE, STAGES>(M, s, active, d, x, sm, epi);
+        epi.end_block(b, d, sm.blk_red);
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.empty[s]);  // this warp is done with stage s
         s = (s + 1 == STAGES) ? 0 : s + 1;
@@ -350,6 +393,7 @@ template <typename X, typename A>
 struct StoreEpi {
     X* __restrict__ y;
     __device__ __forceinline__ void operator()(int32_t row, A v) { y[row] = static_cast<X>(v); }
+    __device__ __forceinline__ void end_block(int64_t, const BlockDesc&, double (*)[kWarps]) {}
 };
 
 // Dynamic shared memory of the pipelined kernels.

@@ -16,7 +16,7 @@ object exporting DLPack / __cuda_array_interface__.
 
 Additions beyond the reference surface are keyword-only or separate names:
 `upload_csr(..., precision="fp32"|"bf16")`, `upload_csr_batched`, `tune`,
-`row_blocks`.
+`tuning`, `autotune`, `row_blocks`.
 """
 from __future__ import annotations
 
@@ -35,7 +35,7 @@ except ImportError:  # pragma: no cover
 __all__ = [
     "init", "finalize", "rank", "size", "barrier", "CrsMatrix", "DistCrsMatrix", "upload_csr",
     "upload_csr_batched", "distribute_csr", "spmv", "batch_spmv", "dist_spmv", "cg_solve",
-    "cg_solve_local", "tune", "tuning", "row_blocks",
+    "cg_solve_local", "tune", "tuning", "autotune", "row_blocks",
 ]
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
@@ -126,9 +126,12 @@ class CrsMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib._lib.nm_csr_destroy(h)
-            self._h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib._lib.nm_csr_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
 
 
 class DistCrsMatrix:
@@ -167,9 +170,12 @@ class DistCrsMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib._lib.nm_dist_destroy(h)
-            self._h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib._lib.nm_dist_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
 
 
 # ---- upload / distribute (src/bindings.cpp:97-148) -----------------------------
@@ -366,6 +372,76 @@ def tune(A: CrsMatrix, tile: int = 0, max_rows: int = 0, short_max: int = 0,
     t = _lib.Tuning(int(tile), int(max_rows), int(short_max), int(grid_mult), int(stages))
     _lib.check(_lib.load().nm_csr_set_tuning(A._h, C.byref(t)), "tune")
     return tuning(A)
+
+
+_TUNE_CACHE: dict = {}
+
+
+def _tune_key(A: CrsMatrix) -> str:
+    # shape, precision and the histogram of per-row reduction bins under the
+    # default partition: matrices with the same key get the same tuning
+    _, bins = row_blocks(A)
+    h = np.bincount(bins.astype(np.int64), minlength=3)
+    return f"{A.nrows}x{A.ncols}:{A.nnz}:{A.precision}:{h[0]}/{h[1]}/{h[2]}"
+
+
+def autotune(A: CrsMatrix, x=None, budget_ms: float = 200.0, cache: bool = True) -> dict:
+    """Choose A's SpMV partition and launch shape by timing candidates on the
+    device (nm_csr_autotune: tile 1024/2048/4096, short_max 32/64, stages
+    2/3/4, grid_mult 0/1/2) and install the fastest.  `x` (optional) is the
+    vector to time with, else U[-1, 1].  Results are cached per matrix
+    signature in-process and, when NUM_B200_TUNE_CACHE names a JSON file,
+    across processes.  Returns the installed tuning plus 'us' (its SpMV time)
+    and 'trials' (every candidate timed; empty on a cache hit)."""
+    import json
+    import os
+    path = os.environ.get("NUM_B200_TUNE_CACHE")
+    tune(A, tile=2048, max_rows=256, short_max=32, grid_mult=0, stages=2)  # key on defaults
+    key = _tune_key(A)
+    if cache:
+        if not _TUNE_CACHE and path and os.path.exists(path):
+            try:
+                with open(path) as f:
+                    _TUNE_CACHE.update(json.load(f))
+            except (OSError, ValueError):
+                pass
+        hit = _TUNE_CACHE.get(key)
+        if hit:
+            t = tune(A, **{k: hit[k] for k in ("tile", "max_rows", "short_max", "grid_mult",
+                                                "stages")})
+            return {**t, "us": hit.get("us"), "trials": [], "cached": True}
+    dt = torch.float64 if A.precision == "fp64" else torch.float32
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if x is None:
+        g = torch.Generator(device=dev).manual_seed(1)
+        xt = torch.rand(A.ncols, dtype=dt, device=dev, generator=g) * 2 - 1
+    else:
+        xt = device_array(x, "float64" if dt == torch.float64 else "float32", "x")
+    y = torch.empty(A.nrows, dtype=dt, device=dev)
+    cap = 64
+    trials = (_lib.TuneTrial * cap)()
+    best = _lib.Tuning()
+    nt = C.c_int32(0)
+    s = stream_of(y)
+    _lib.check(_lib.load().nm_csr_autotune(A._h, xt.data_ptr(), y.data_ptr(), s,
+                                           float(budget_ms), C.byref(best), trials, cap,
+                                           C.byref(nt)), "autotune")
+    out = []
+    for t in trials[: min(cap, nt.value)]:
+        out.append({"tile": t.tuning.tile, "short_max": t.tuning.short_max,
+                    "stages": t.tuning.stages, "grid_mult": t.tuning.grid_mult,
+                    "us": round(float(t.us), 3)})
+    res = tuning(A)
+    us = min(o["us"] for o in out) if out else None
+    if cache:
+        _TUNE_CACHE[key] = {**res, "us": us}
+        if path:
+            try:
+                with open(path, "w") as f:
+                    json.dump(_TUNE_CACHE, f, indent=1, sort_keys=True)
+            except OSError:
+                pass
+    return {**res, "us": us, "trials": out, "cached": False}
 
 
 def row_blocks(A: CrsMatrix):

@@ -241,3 +241,30 @@ def test_staged_x_ragged_columns(kspmv, oracle, tile):
     scale = oracle.spmv(A.row_ptr, A.col_idx, np.abs(A.values).astype(np.float32),
                         np.abs(x).astype(np.float32))
     assert np.all(np.abs(y32 - ref32) <= TOL32 * scale)
+
+
+def test_autotune_installs_a_valid_tuning(kspmv, oracle, tmp_path, monkeypatch):
+    # The autotuner times every candidate, installs the fastest, and the
+    # product under the chosen partition keeps the bar (rows of <= 32
+    # nonzeros stay thread-per-row: bit-exact).  A second call hits the cache.
+    monkeypatch.setenv("NUM_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    kspmv._TUNE_CACHE.clear()
+    A = gen.power_law(200_000, seed=1001)
+    x = np.random.default_rng(1).uniform(-1, 1, A.ncols)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    res = kspmv.autotune(M, budget_ms=50)
+    assert not res["cached"] and len(res["trials"]) >= 20
+    assert res["tile"] in (1024, 2048, 4096) and res["short_max"] in (32, 64)
+    assert res["stages"] in (2, 3, 4) and res["grid_mult"] in (0, 1, 2)
+    assert res["us"] == min(t["us"] for t in res["trials"])
+    assert {k: res[k] for k in ("tile", "short_max", "stages", "grid_mult")} == \
+        {k: kspmv.tuning(M)[k] for k in ("tile", "short_max", "stages", "grid_mult")}
+    xt = torch.tensor(x, device="cuda")
+    yt = torch.full((A.nrows,), float("nan"), dtype=torch.float64, device="cuda")
+    kspmv.spmv(M, xt, yt)
+    _, bins = kspmv.row_blocks(M)
+    _check64(oracle, A, x, yt.cpu().numpy(), bins)
+    assert json.loads((tmp_path / "tune.json").read_text())
+    kspmv._TUNE_CACHE.clear()
+    again = kspmv.autotune(M, budget_ms=50)
+    assert again["cached"] and again["tile"] == res["tile"] and again["stages"] == res["stages"]
