@@ -240,8 +240,9 @@ int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t* const* row
                           int32_t* slots, int32_t* admitted);
 
 /* One step of the batch: the pending refinement steps, then `iters` inner
- * iterations of every active system, then the systems' states are read back;
- * *n_done = systems that finished in this step.  Synchronous. */
+ * iterations of every active system (rounded up to an even count), then the
+ * systems' states are read back; *n_done = systems that finished in this
+ * step.  Synchronous. */
 int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done);
 
 /* Engine counters since creation: steps run, list rebuilds, chunk graph

@@ -64,6 +64,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // Row epilogue of K1: store Ap and accumulate p.Ap.
 struct PApEpi {
+    static constexpr bool kBlockSums = false;
     double* __restrict__ Ap;
     const double* __restrict__ p;
     double dot;
@@ -71,7 +72,8 @@ struct PApEpi {
         Ap[row] = v;
         dot = fma(__ldg(p + row), v, dot);
     }
-    __device__ __forceinline__ void end_block(int64_t, const BlockDesc&, double (*)[kWarps]) {}
+    __device__ __forceinline__ double take() { return 0.0; }
+    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
 };
 
 template <int TILE, int STAGES>

@@ -54,7 +54,8 @@ struct SysState {
     // dynamic
     int32_t phase, it_total, it_inner, outer;
     int32_t converged, pad_;
-    double rnorm, rz, rr0, rr, alpha, beta, final_res;
+    double rnorm, rr0, rr, beta, final_res;
+    double rzp[2];  // r.z of the current inner iteration, alternating by iteration parity
 };
 
 struct SysRef {
@@ -66,7 +67,7 @@ struct ListHdr {
     int32_t iblk, itile, isys, oblk, otile, osys, pad_[2];
 };
 
-constexpr int kTileRows = 1024;  // rows per vector-kernel tile (within one system)
+constexpr int kTileRows = 2048;  // rows per vector-kernel tile (within one system)
 
 __device__ __forceinline__ int32_t sys_phase(const SysState* sys, int32_t slot) {
     return __ldcg(&sys[slot].phase);
@@ -74,69 +75,31 @@ __device__ __forceinline__ int32_t sys_phase(const SysState* sys, int32_t slot) 
 
 // ---- SpMV epilogues / gates ---------------------------------------------------
 
-// Sum of part[lo, hi) by one warp in a fixed order (lane-strided, 8
-// independent accumulators by relative index, then the shuffle tree): the
-// same grouping wherever the range sits; valid in every lane.
-__device__ __forceinline__ double warp_ordered_sum(const double* part, int64_t lo, int64_t hi) {
-    const int lane = threadIdx.x & 31;
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t i = lo + lane;
-    for (; i + 7 * 32 < hi; i += 8 * 32) {
-        double v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = __ldcg(part + i + k * 32);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) a[k] += v[k];
-    }
-    for (int k = 0; i < hi; i += 32, ++k) a[k] += __ldcg(part + i);
-    double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-// Ap = A p.  Per block: the sum of p.Ap over its rows; the warp whose block
-// arrives last for its system sums that system's block sums in block order
-// and sets alpha = r.z / p.Ap.
+// Ap = A p; per row block, the sum of p.Ap over its rows goes to part[b] (the
+// block's consumer warps' sums, added in warp order by the producer warp).
 template <typename T>
 struct InnerEpi {
+    static constexpr bool kBlockSums = true;
     T* __restrict__ Ap;
     const T* __restrict__ p;
     double* __restrict__ part;
-    unsigned int* __restrict__ cnt;  // per slot: blocks arrived this launch
-    const int2* __restrict__ sblk;   // per slot: its block range in the list
-    SysState* sys;
     T acc;
     __device__ __forceinline__ void operator()(int32_t row, T v) {
         Ap[row] = v;
         acc += __ldg(p + row) * v;
     }
-    __device__ __forceinline__ void end_block(int64_t b, const BlockDesc& d,
-                                              double (*buf)[kWarps]) {
-        consumer_block_sum(double(acc), buf, b, part + b);
+    __device__ __forceinline__ double take() {
+        const double a = double(acc);
         acc = T(0);
-        if ((threadIdx.x >> 5) != 0) return;  // warp 0 finalises
-        const int lane = threadIdx.x & 31;
-        const int32_t slot = d.aux.y;
-        const int2 range = __ldg(sblk + slot);
-        int last = 0;
-        if (lane == 0) {
-            __threadfence();  // this block's sum before the arrival
-            last = atomicAdd(cnt + slot, 1u) == unsigned(range.y - range.x - 1);
-        }
-        last = __shfl_sync(0xffffffffu, last, 0);
-        if (!last) return;
-        __threadfence();
-        const double pAp = warp_ordered_sum(part, range.x, range.y);
-        if (lane == 0) {
-            cnt[slot] = 0u;
-            SysState& S = sys[slot];
-            if (S.phase == kSysInner) S.alpha = (pAp != 0.0) ? S.rz / pAp : 0.0;
-        }
+        return a;
+    }
+    __device__ __forceinline__ void finish_block(int64_t b, const BlockDesc&, double sum) {
+        part[b] = sum;
     }
 };
 
-struct OuterEpi {  // r64 = b - A x, per-warp partials of r64.r64
+struct OuterEpi {  // r64 = b - A x; per row block, the sum of r64.r64 -> part[b]
+    static constexpr bool kBlockSums = true;
     double* __restrict__ r64;
     const double* __restrict__ b;
     double* __restrict__ part;
@@ -146,10 +109,13 @@ struct OuterEpi {  // r64 = b - A x, per-warp partials of r64.r64
         r64[row] = r;
         acc = fma(r, r, acc);
     }
-    __device__ __forceinline__ void end_block(int64_t b, const BlockDesc&,
-                                              double (*buf)[kWarps]) {
-        consumer_block_sum(acc, buf, b, part + b);
+    __device__ __forceinline__ double take() {
+        const double a = acc;
         acc = 0.0;
+        return a;
+    }
+    __device__ __forceinline__ void finish_block(int64_t bb, const BlockDesc&, double sum) {
+        part[bb] = sum;
     }
 };
 
@@ -166,11 +132,11 @@ constexpr int kSolverStages = 2;
 
 template <typename V, typename T>
 __global__ void __launch_bounds__(kCtaThreads)
-    bs_spmv_inner(CsrView<V> M, const T* __restrict__ p, T* __restrict__ Ap, SysState* sys,
-                  double* part, unsigned int* cnt, const int2* sblk, unsigned int* err) {
+    bs_spmv_inner(CsrView<V> M, const T* __restrict__ p, T* __restrict__ Ap, const SysState* sys,
+                  double* part, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<SpmvSmem<V, T, T, kSolverTile, kSolverStages>*>(smem_raw);
-    InnerEpi<T> epi{Ap, p, part, cnt, sblk, sys, T(0)};
+    InnerEpi<T> epi{Ap, p, part, T(0)};
     spmv_pipeline<V, T, T, kSolverTile, kSolverStages>(M, p, sm, epi, err,
                                                        PhaseGate{sys, kSysInner});
 }
@@ -186,39 +152,83 @@ __global__ void __launch_bounds__(kCtaThreads)
                                                                       PhaseGate{sys, kSysOuter});
 }
 
-// ---- per-system scalar steps -------------------------------------------------------
+// ---- fixed-order reductions ---------------------------------------------------------
+
+// CTA-wide sums of two values in a fixed order (shuffle tree per warp, warps
+// in order), returned to every thread.  scratch: one entry per warp plus one
+// for the result (which no warp slot overlaps, so back-to-back calls need no
+// third barrier).
+__device__ __forceinline__ double2 block_sum2_all(double a, double b, double2* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = static_cast<int>(blockDim.x) >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) scratch[warp] = make_double2(a, b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nw; ++w) {
+            t.x += scratch[w].x;
+            t.y += scratch[w].y;
+        }
+        scratch[nw] = t;
+    }
+    __syncthreads();
+    return scratch[nw];
+}
+
+// Sums of the pairs part[lo..hi) (as double2: .x and .y summed separately), or
+// of single values when PAIRS is false (.y = 0), returned to every thread.
+// Thread t owns the entries lo + t + k*blockDim (k = 0, 1, ...) and adds them
+// into 8 accumulators by k % 8, combined as ((0+1)+(2+3))+((4+5)+(6+7)); then
+// the CTA sum above.  The grouping depends only on the offset from lo, so a
+// system's sums are the same bits wherever its entries sit and in every CTA
+// that computes them.
+template <bool PAIRS>
+__device__ __forceinline__ double2 ordered_sum_all(const double* part, int64_t lo, int64_t hi,
+                                                   double2* scratch) {
+    double ax[8] = {0, 0, 0, 0, 0, 0, 0, 0}, ay[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int64_t bs = blockDim.x;
+    auto ld = [&](int64_t i) -> double2 {
+        if (PAIRS) return __ldcg(reinterpret_cast<const double2*>(part) + i);
+        return make_double2(__ldcg(part + i), 0.0);
+    };
+    int64_t i = lo + threadIdx.x;
+    for (; i + 7 * bs < hi; i += 8 * bs) {
+        double2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = ld(i + k * bs);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            ax[k] += v[k].x;
+            ay[k] += v[k].y;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {  // the tail: fewer than 8 strides remain
+        const int64_t j = i + k * bs;
+        if (j < hi) {
+            const double2 v = ld(j);
+            ax[k] += v.x;
+            ay[k] += v.y;
+        }
+    }
+    const double sx = ((ax[0] + ax[1]) + (ax[2] + ax[3])) + ((ax[4] + ax[5]) + (ax[6] + ax[7]));
+    const double sy = ((ay[0] + ay[1]) + (ay[2] + ay[3])) + ((ay[4] + ay[5]) + (ay[6] + ay[7]));
+    return block_sum2_all(sx, sy, scratch);
+}
+
+// ---- per-system scalar steps (one CTA per system of the outer list) ----------------
 
 enum ScalarKind { kOuterNorm = 2, kStart = 3 };
 
 constexpr int kScalarThreads = 1024;
 
-// Sum of part[lo, hi) (stride `step`, offset `off`) in a fixed order; valid in
-// thread 0.  Thread t owns the entries lo + t + k*blockDim (k = 0, 1, ...),
-// summed with 8 independent accumulators (entry k goes to accumulator k % 8)
-// that are then added in order -- the same grouping for any lo, so a system's
-// sums do not depend on where its entries sit in the list.
-__device__ __forceinline__ double ordered_sum(const double* part, int64_t lo, int64_t hi,
-                                              int step, int off, double* red) {
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int64_t bs = blockDim.x;
-    int64_t i = lo + threadIdx.x;
-    for (; i + 7 * bs < hi; i += 8 * bs) {
-        double v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = __ldcg(part + (i + k * bs) * step + off);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) a[k] += v[k];
-    }
-    for (int k = 0; i < hi; i += bs, ++k) a[k] += __ldcg(part + i * step + off);
-    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-    return block_sum(s, red);
-}
-
 template <int KIND>
 __global__ void __launch_bounds__(kScalarThreads)
     bs_scalar(const SysRef* list, const int32_t* count, SysState* sys, const double* part_blk,
               const double* part_tile) {
-    __shared__ double red[kScalarThreads / 32];
+    __shared__ double2 red[kScalarThreads / 32 + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const SysRef ref = list[i];
@@ -226,7 +236,7 @@ __global__ void __launch_bounds__(kScalarThreads)
         const int32_t ph = __ldcg(&S.phase);
         if (ph != kSysOuter) continue;  // uniform over the CTA
         if (KIND == kOuterNorm) {
-            const double rr = ordered_sum(part_blk, ref.blk0, ref.blk1, 1, 0, red);
+            const double rr = ordered_sum_all<false>(part_blk, ref.blk0, ref.blk1, red).x;
             if (threadIdx.x == 0) {
                 const double rnorm = sqrt(rr);
                 const double res = rnorm / S.bnorm;
@@ -243,20 +253,64 @@ __global__ void __launch_bounds__(kScalarThreads)
                 }
             }
         } else {  // kStart
-            const double rz = ordered_sum(part_tile, ref.tile0, ref.tile1, 2, 0, red);
-            const double rr = ordered_sum(part_tile, ref.tile0, ref.tile1, 2, 1, red);
+            const double2 t = ordered_sum_all<true>(part_tile, ref.tile0, ref.tile1, red);
             if (threadIdx.x == 0) {
-                S.rz = rz;
-                S.rr0 = rr > 0.0 ? rr : 1.0;
-                S.rr = rr;
+                S.rzp[0] = t.x;
+                S.rzp[1] = t.x;
+                S.rr0 = t.y > 0.0 ? t.y : 1.0;
+                S.rr = t.y;
                 S.it_inner = 0;
                 S.phase = kSysInner;
             }
         }
+        __syncthreads();  // red is reused by the next system
     }
 }
 
 // ---- per-row vector steps over tiles {row0, row1, slot} ----------------------------
+//
+// A tile is up to kTileRows consecutive rows of one system; tiles start on
+// multiples of 4 rows (systems start on multiples of 4 and tiles are
+// kTileRows apart).  Thread t handles the vectors of VN = 16 / sizeof(T)
+// rows starting at row0 + VN*(t + k*blockDim).  A vector may reach past the
+// system's last row into its own padding rows (each system owns at least one
+// row beyond its end, rounded up to 4): those lanes are loaded but neither
+// stored nor counted.
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int N = 4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int N = 2;
+};
+
+template <typename T>
+__device__ __forceinline__ void vload(const T* p, int64_t row, T (&v)[Vec16<T>::N]) {
+    using VT = typename Vec16<T>::type;
+    const VT q = *reinterpret_cast<const VT*>(p + row);
+    memcpy(v, &q, sizeof q);
+}
+
+template <typename T>
+__device__ __forceinline__ void vstore(T* p, int64_t row, const T (&v)[Vec16<T>::N], int valid) {
+    using VT = typename Vec16<T>::type;
+    constexpr int N = Vec16<T>::N;
+    if (valid >= N) {
+        VT q;
+        memcpy(&q, v, sizeof q);
+        *reinterpret_cast<VT*>(p + row) = q;
+    } else {
+#pragma unroll
+        for (int e = 0; e < N; ++e)
+            if (e < valid) p[row + e] = v[e];
+    }
+}
 
 // x += d * rnorm (the inner solution solves A d = r64 / rnorm), before the outer SpMV.
 template <typename T>
@@ -280,7 +334,7 @@ __global__ void __launch_bounds__(kThreads)
     bs_inner_start(const int4* tiles, const int32_t* count, const SysState* sys,
                    const double* __restrict__ r64, const T* __restrict__ dinv, T* __restrict__ r,
                    T* __restrict__ z, T* __restrict__ p, T* __restrict__ d, double* part) {
-    __shared__ double red[kWarps];
+    __shared__ double2 red[kWarps + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const int4 tl = tiles[i];
@@ -299,90 +353,145 @@ __global__ void __launch_bounds__(kThreads)
                 rr += ri * ri;
             }
         }
-        const double s0 = block_sum(double(rz), red);
-        const double s1 = block_sum(double(rr), red);
-        if (threadIdx.x == 0) {
-            part[2 * int64_t(i)] = s0;
-            part[2 * int64_t(i) + 1] = s1;
-        }
+        const double2 t = block_sum2_all(double(rz), double(rr), red);
+        if (threadIdx.x == 0) reinterpret_cast<double2*>(part)[i] = t;
     }
 }
 
-// d += alpha p, r -= alpha Ap, z = M^-1 r; one CTA per tile writes the tile's
-// (r.z, r.r); the CTA whose tile arrives last for its system sums the system's
-// tile sums in tile order and runs the inner stopping test and beta.
+__host__ __device__ constexpr int kVecIters(int vn) { return kTileRows / (vn * kThreads); }
+
+// Inner iteration, step 2 (after the SpMV): alpha = r.z / p.Ap from the
+// system's block sums (every CTA of the system sums them, in the same order),
+// d += alpha p, r -= alpha Ap, z = M^-1 r, and the tile's (r.z, r.r) -> part.
+// The system's first tile counts the iteration.  No atomics: step 3 reduces
+// the tile sums.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-    bs_update(const int4* tiles, const int32_t* count, SysState* sys, const T* __restrict__ p,
+    bs_update(const int4* tiles, const int32_t* count, SysState* sys, const int2* sblk,
+              const int2* stile, const double* part_blk, const T* __restrict__ p,
               const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
-              T* __restrict__ z, T* __restrict__ d, double* part, unsigned int* cnt,
-              const int2* stile) {
-    __shared__ double red[kWarps];
-    __shared__ int last;
+              T* __restrict__ z, T* __restrict__ d, double* part_tile, int par) {
+    constexpr int VN = Vec16<T>::N;
+    constexpr int IT = kVecIters(VN);
+    __shared__ double2 red[kWarps + 1];
     const int32_t i = blockIdx.x;
     if (i >= __ldcg(count)) return;
     const int4 tl = tiles[i];
     const int32_t slot = tl.z;
-    const bool live = sys_phase(sys, slot) == kSysInner;
     T rz = T(0), rr = T(0);
-    if (live) {
-        const T alpha = T(__ldcg(&sys[slot].alpha));
-        for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x) {
-            const T pi = p[row];
-            d[row] = fma(alpha, pi, d[row]);
-            const T ri = fma(-alpha, Ap[row], r[row]);
-            const T zi = dinv[row] * ri;
-            r[row] = ri;
-            z[row] = zi;
-            rz = fma(ri, zi, rz);
-            rr = fma(ri, ri, rr);
+    if (sys_phase(sys, slot) == kSysInner) {  // phase is not written by this kernel
+        // operands first, so their latency overlaps the block-sum reduction
+        T pv[IT][VN], av[IT][VN], rv[IT][VN], dv[IT][VN], mv[IT][VN];
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
+            if (row < tl.y) {
+                vload(p, row, pv[k]);
+                vload(Ap, row, av[k]);
+                vload(r, row, rv[k]);
+                vload(d, row, dv[k]);
+                vload(dinv, row, mv[k]);
+            }
+        }
+        const int2 br = __ldg(sblk + slot);
+        const double pAp = ordered_sum_all<false>(part_blk, br.x, br.y, red).x;
+        const double rz_old = __ldcg(&sys[slot].rzp[par]);
+        const T alpha = T(pAp != 0.0 ? rz_old / pAp : 0.0);
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
+            if (row < tl.y) {
+                const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
+                T zo[VN];
+#pragma unroll
+                for (int e = 0; e < VN; ++e) {
+                    dv[k][e] = fma(alpha, pv[k][e], dv[k][e]);
+                    rv[k][e] = fma(-alpha, av[k][e], rv[k][e]);
+                    zo[e] = mv[k][e] * rv[k][e];
+                    if (e < valid) {
+                        rz = fma(rv[k][e], zo[e], rz);
+                        rr = fma(rv[k][e], rv[k][e], rr);
+                    }
+                }
+                vstore(d, row, dv[k], valid);
+                vstore(r, row, rv[k], valid);
+                vstore(z, row, zo, valid);
+            }
+        }
+        if (threadIdx.x == 0 && i == __ldg(stile + slot).x) {
+            sys[slot].it_inner += 1;
+            sys[slot].it_total += 1;
         }
     }
-    const double s0 = block_sum(double(rz), red);
-    const double s1 = block_sum(double(rr), red);
-    const int2 range = __ldg(stile + slot);
-    if (threadIdx.x == 0) {
-        part[2 * int64_t(i)] = s0;
-        part[2 * int64_t(i) + 1] = s1;
-        __threadfence();
-        last = atomicAdd(cnt + slot, 1u) == unsigned(range.y - range.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    const double rzn = ordered_sum(part, range.x, range.y, 2, 0, red);
-    const double rrn = ordered_sum(part, range.x, range.y, 2, 1, red);
-    if (threadIdx.x == 0) {
-        cnt[slot] = 0u;
-        SysState& S = sys[slot];
-        if (!live) return;
-        S.it_inner += 1;
-        S.it_total += 1;
-        S.rr = rrn;
-        const double inner_rel = sqrt(rrn / S.rr0);
-        const double est = S.rnorm * sqrt(rrn) / S.bnorm;  // estimated |b - Ax| / |b|
-        if (!(inner_rel > S.inner_rtol) || !(est >= S.stop_frac * S.tol) ||
-            S.it_total >= S.max_iter) {
-            S.phase = kSysOuter;  // stop the inner solve; refine next step
-        } else {
-            S.beta = rzn / S.rz;
-            S.rz = rzn;
-        }
-    }
+    const double2 t = block_sum2_all(double(rz), double(rr), red);
+    if (threadIdx.x == 0) reinterpret_cast<double2*>(part_tile)[i] = t;
 }
 
-// p = z + beta p.
+// Inner iteration, step 3: (r.z, r.r) of the system from its tile sums
+// (every CTA, same order); the inner stopping test; p = z + beta p with
+// beta = r.z / previous r.z.  r.z alternates between rzp[par] (read) and
+// rzp[par ^ 1] (written by the system's first tile), so no CTA reads a value
+// another CTA of this launch writes; the phase change of a stopping system is
+// the one write others may see early, and they then skip exactly as the test
+// would make them.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-    bs_pupdate(const int4* tiles, const int32_t* count, const SysState* sys,
-               const T* __restrict__ z, T* __restrict__ p) {
-    const int32_t n = __ldcg(count);
-    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
-        const int4 tl = tiles[i];
-        if (sys_phase(sys, tl.z) != kSysInner) continue;
-        const T beta = T(__ldcg(&sys[tl.z].beta));
-        for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x)
-            p[row] = fma(beta, p[row], z[row]);
+    bs_pupdate(const int4* tiles, const int32_t* count, SysState* sys, const int2* stile,
+               const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par) {
+    constexpr int VN = Vec16<T>::N;
+    constexpr int IT = kVecIters(VN);
+    __shared__ double2 red[kWarps + 1];
+    __shared__ int32_t phase;
+    const int32_t i = blockIdx.x;
+    if (i >= __ldcg(count)) return;
+    const int4 tl = tiles[i];
+    const int32_t slot = tl.z;
+    if (threadIdx.x == 0) phase = sys_phase(sys, slot);
+    __syncthreads();
+    if (phase != kSysInner) return;  // uniform over the CTA
+    T zv[IT][VN], pv[IT][VN];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
+        if (row < tl.y) {
+            vload(z, row, zv[k]);
+            vload(p, row, pv[k]);
+        }
+    }
+    const int2 tr = __ldg(stile + slot);
+    const double2 t = ordered_sum_all<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
+    const SysState& S = sys[slot];
+    const double rr0 = __ldcg(&S.rr0), rnorm = __ldcg(&S.rnorm), bnorm = __ldcg(&S.bnorm);
+    const double inner_rel = sqrt(t.y / rr0);
+    const double est = rnorm * sqrt(t.y) / bnorm;  // estimated |b - Ax| / |b|
+    const bool stop = !(inner_rel > __ldcg(&S.inner_rtol)) ||
+                      !(est >= __ldcg(&S.stop_frac) * __ldcg(&S.tol)) ||
+                      __ldcg(&S.it_total) >= __ldcg(&S.max_iter);
+    const bool first = i == tr.x;
+    if (stop) {  // stop the inner solve; refine next step
+        if (first && threadIdx.x == 0) {
+            sys[slot].rr = t.y;
+            sys[slot].phase = kSysOuter;
+        }
+        return;
+    }
+    const double rz_old = __ldcg(&S.rzp[par]);
+    const double beta_d = t.x / rz_old;
+    const T beta = T(beta_d);
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
+        if (row < tl.y) {
+            const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
+#pragma unroll
+            for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
+            vstore(p, row, pv[k], valid);
+        }
+    }
+    if (first && threadIdx.x == 0) {
+        sys[slot].rr = t.y;
+        sys[slot].beta = beta_d;
+        sys[slot].rzp[par ^ 1] = t.x;
     }
 }
 
@@ -469,7 +578,6 @@ struct nm_solver {
     nm::SysRef *isys = nullptr, *osys = nullptr;
     int64_t cap_blk = 0, cap_tile = 0;
     double *part_blk = nullptr, *part_tile = nullptr;
-    unsigned int *cnt_blk = nullptr, *cnt_tile = nullptr;  // per slot arrival counters
     int2 *sblk = nullptr, *stile = nullptr;                // per slot ranges in the inner lists
     int2 *h_sblk = nullptr, *h_stile = nullptr;
     nm::BlockDesc* h_blk = nullptr;  // pinned staging (iblk then oblk)
@@ -500,7 +608,7 @@ nm_solver::~nm_solver() {
     cudaFree(hdr); cudaFreeHost(h_hdr);
     cudaFree(iblk); cudaFree(oblk); cudaFree(itile); cudaFree(otile); cudaFree(isys); cudaFree(osys);
     cudaFree(part_blk); cudaFree(part_tile);
-    cudaFree(cnt_blk); cudaFree(cnt_tile); cudaFree(sblk); cudaFree(stile);
+    cudaFree(sblk); cudaFree(stile);
     cudaFreeHost(h_sblk); cudaFreeHost(h_stile);
     cudaFreeHost(h_blk); cudaFreeHost(h_tile); cudaFreeHost(h_ref); cudaFreeHost(stage);
     if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
@@ -659,12 +767,16 @@ int launch_inner_iters(nm_solver* S, int iters) {
     T* z = static_cast<T*>(S->z);
     T* d = static_cast<T*>(S->d);
     const T* dinv = static_cast<const T*>(S->dinv);
+    // iters is even, so the r.z parity of every chunk starts at 0
     for (int it = 0; it < iters; ++it) {
+        const int par = it & 1;
         bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
-                                                              S->cnt_blk, S->sblk, S->err);
-        bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, p, Ap, dinv, r, z, d,
-                                                S->part_tile, S->cnt_tile, S->stile);
-        bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, z, p);
+                                                              S->err);
+        bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->sblk, S->stile,
+                                                S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
+                                                par);
+        bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
+                                                 S->part_tile, z, p, par);
     }
     NM_CHECK_LAUNCH();
     return NM_OK;
@@ -785,10 +897,6 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     NM_CUDA_TRY(cudaMalloc(&S->isys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->osys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 2));
-    for (unsigned int** c : {&S->cnt_blk, &S->cnt_tile}) {
-        NM_CUDA_TRY(cudaMalloc(c, sizeof(unsigned int) * size_t(max_systems)));
-        NM_CUDA_TRY(cudaMemset(*c, 0, sizeof(unsigned int) * size_t(max_systems)));
-    }
     for (int2** r : {&S->sblk, &S->stile}) {
         NM_CUDA_TRY(cudaMalloc(r, sizeof(int2) * size_t(max_systems)));
         NM_CUDA_TRY(cudaMemset(*r, 0, sizeof(int2) * size_t(max_systems)));
@@ -1183,6 +1291,8 @@ extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
     using clk = std::chrono::steady_clock;
     clear_error();
     if (!S) return fail(NM_ERR_INVALID, "nm_solver_step: NULL solver");
+    if (iters < 0) return fail(NM_ERR_INVALID, "nm_solver_step: iters must be >= 0");
+    iters = (iters + 1) & ~1;  // whole pairs (the r.z double buffer alternates)
     int st = NM_OK;
     auto t0 = clk::now();
     auto lap = [&t0](double& acc) {

@@ -24,6 +24,11 @@
 //
 // The epilogue functor receives (row, value) exactly once per row, on one
 // consumer thread; CG uses it to store Ap and to accumulate p.Ap on the fly.
+// An epilogue with kBlockSums also gets one sum per row block: each consumer
+// warp reduces its threads' take() values and parks the warp's sum in the
+// stage's slot before releasing the stage; the producer, once the stage is
+// released, adds the eight warp sums in warp order and hands the block sum to
+// finish_block(b, d, sum) -- no barrier or atomic on the consumers' path.
 //
 // Alignment (TMA bulk copies need 16-byte aligned addresses and sizes): the
 // staged nonzero range is [z0 & ~7, (z1 + 7) & ~7), the row_ptr range
@@ -102,28 +107,9 @@ struct SpmvSmem {
     int32_t long_rows[kThreads];
     int32_t warp_cnt[kWarps];
     A red[kWarps + 1];
-    double blk_red[2][kWarps];  // per-block epilogue sums, double-buffered by block parity
+    double blk_red[STAGES][kWarps];  // per-warp epilogue sums of the block in each stage
+    int64_t bid[STAGES];             // index of the block in each stage
 };
-
-// Per-block sum of one value per consumer thread, in a fixed order (warp
-// shuffle tree, then warps 0..7), written by consumer thread 0 to *out.  One
-// consumer barrier; the two buffers alternate with the block's parity, which
-// makes a second barrier unnecessary (a warp can only write a buffer again
-// after the barrier of the next block, which thread 0 reaches after reading).
-__device__ __forceinline__ void consumer_block_sum(double v, double (*buf)[kWarps],
-                                                   int64_t parity, double* out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_sum(v);
-    double* b = buf[parity & 1];
-    if (lane == 0) b[warp] = v;
-    consumer_sync();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) s += b[w];
-        *out = s;
-    }
-}
 
 __device__ __forceinline__ BlockDesc load_desc(const BlockDesc* p) {
     const int4* q = reinterpret_cast<const int4*>(p);
@@ -330,6 +316,15 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
             dd.aux.z = gate(dd) ? 0 : 1;
             return dd;
         };
+        // the block sum of the (released) block in stage q, to the epilogue
+        auto finish = [&](int q) {
+            if constexpr (Epi::kBlockSums) {
+                double sum = 0.0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) sum += sm.blk_red[q][w];
+                epi.finish_block(sm.bid[q], sm.meta[q], sum);
+            }
+        };
         BlockDesc next{};
         if (int64_t(blockIdx.x) < M.nblk) next = fetch(blockIdx.x);
         for (int64_t b = blockIdx.x; b < M.nblk; b += gridDim.x, ++k) {
@@ -342,11 +337,25 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
                     break;
                 }
                 empty_par ^= 1u << s;
+                finish(s);
             }
+            sm.bid[s] = b;
             spmv_issue<V, X, A, TILE, STAGES>(M, x, d, sm, s);
             full_par ^= 1u << s;
             used |= 1u << s;
             s = (s + 1 == STAGES) ? 0 : s + 1;
+        }
+        if constexpr (Epi::kBlockSums) {
+            // the blocks still in the ring: wait for their release, finish them
+            for (int q = 0; ok && q < STAGES; ++q) {
+                if (!(used & (1u << q))) continue;
+                if (!mbar_wait_bounded(&sm.empty[q], (empty_par >> q) & 1u)) {
+                    atomicOr(err, kErrWaitTimeout);
+                    ok = false;
+                    break;
+                }
+                finish(q);
+            }
         }
         // Drain: every stage's last copy has landed before the CTA may exit.
         for (int q = 0; q < STAGES; ++q)
@@ -380,7 +389,10 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
             spmv_long_row<V, X, A, TILE, STAGES>(M, active, d.rz.x, d.rz.z, d.rz.w, x, sm, epi);
         else
             spmv_rows<V, X, A, TILE, STAGES>(M, s, active, d, x, sm, epi);
-        epi.end_block(b, d, sm.blk_red);
+        if constexpr (Epi::kBlockSums) {
+            const double v = warp_sum(epi.take());
+            if (lane == 0) sm.blk_red[s][warp] = v;  // published by the arrival below
+        }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.empty[s]);  // this warp is done with stage s
         s = (s + 1 == STAGES) ? 0 : s + 1;
@@ -391,9 +403,11 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
 // Epilogue: y[row] = value.
 template <typename X, typename A>
 struct StoreEpi {
+    static constexpr bool kBlockSums = false;
     X* __restrict__ y;
     __device__ __forceinline__ void operator()(int32_t row, A v) { y[row] = static_cast<X>(v); }
-    __device__ __forceinline__ void end_block(int64_t, const BlockDesc&, double (*)[kWarps]) {}
+    __device__ __forceinline__ double take() { return 0.0; }
+    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
 };
 
 // Dynamic shared memory of the pipelined kernels.
