@@ -245,15 +245,25 @@ int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t* const* row
  * step.  Synchronous. */
 int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done);
 
+/* nm_solver_step in two halves, so that host work overlaps the device:
+ * _begin enqueues the step and returns; nm_solver_admit / _admit_batch may run
+ * meanwhile (their host preparation overlaps the iterations, their uploads go
+ * on a separate stream; the systems join at the next step); _end waits and
+ * reads the states back.  nm_solver_take is refused between the two. */
+int nm_solver_step_begin(nm_solver* S, int32_t iters);
+int nm_solver_step_end(nm_solver* S, int32_t* n_done);
+
 /* Engine counters since creation: steps run, list rebuilds, chunk graph
  * captures and full instantiations, outer (refinement) launches, inner
- * iterations enqueued, and host seconds spent per part of nm_solver_step
- * (list upload, outer launch, capture, graph run + state read-back, state
- * scan). */
+ * iterations enqueued; host seconds spent per part of a step (list upload,
+ * outer launch, capture, waiting in nm_solver_step_end, state scan) and of
+ * admission (parallel preparation, upload enqueue); device seconds of all
+ * steps and milliseconds of the last one. */
 typedef struct {
     int64_t steps, list_uploads, graph_captures, graph_instantiations, outer_launches,
         inner_iterations;
     double s_lists, s_outer, s_capture, s_run, s_scan;
+    double s_admit_prep, s_admit_commit, s_device, last_step_ms;
 } nm_solver_counters;
 int nm_solver_counters_get(const nm_solver* S, nm_solver_counters* out);
 

@@ -40,7 +40,9 @@ class SolverCounters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "list_uploads", "graph_captures",
                                          "graph_instantiations", "outer_launches",
                                          "inner_iterations")] + \
-               [(n, C.c_double) for n in ("s_lists", "s_outer", "s_capture", "s_run", "s_scan")]
+               [(n, C.c_double) for n in ("s_lists", "s_outer", "s_capture", "s_run", "s_scan",
+                                          "s_admit_prep", "s_admit_commit", "s_device",
+                                          "last_step_ms")]
 
 
 class TuneTrial(C.Structure):
@@ -79,6 +81,8 @@ _SIGNATURES = {
     "nm_solver_admit": ([vp, vp, vp, vp, i32, vp, vp, dbl, i32, P_i32], C.c_int),
     "nm_solver_admit_batch": ([vp, i32, vp, vp, vp, vp, vp, dbl, i32, P_i32, P_i32], C.c_int),
     "nm_solver_step": ([vp, i32, P_i32], C.c_int),
+    "nm_solver_step_begin": ([vp, i32], C.c_int),
+    "nm_solver_step_end": ([vp, P_i32], C.c_int),
     "nm_solver_counters_get": ([vp, vp], C.c_int),
     "nm_solver_status": ([vp, i32, P_i32, C.POINTER(CgResult), P_i32], C.c_int),
     "nm_solver_take": ([vp, i32, vp], C.c_int),

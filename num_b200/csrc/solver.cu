@@ -26,8 +26,11 @@
 //   residual system A d = r64 / |r64|; an outer step (x += d |r64|,
 //   r64 = b - A x with FP64 values, fused into the FP64 SpMV's epilogue,
 //   |r64| / |b|) runs between chunks for systems whose inner solve stopped,
-//   until |b - A x| / |b| < tol.  With T = double the same machinery is a
-//   plain FP64 PCG (the inner test is the final one).
+//   until |b - A x| / |b| < tol.  From the second outer step on, the inner
+//   solve continues the previous Krylov direction instead of restarting
+//   ("reliable update": the true residual replaces the recurred one, p = z +
+//   gamma p), so refinement costs few extra iterations.  With T = double the
+//   same machinery is a plain FP64 PCG (the inner test is the final one).
 //
 // * Continuous batching.  nm_solver_step runs the pending outer steps, then a
 //   chunk of inner iterations, then reads every system's state; the host
@@ -38,6 +41,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -55,7 +59,10 @@ struct SysState {
     int32_t phase, it_total, it_inner, outer;
     int32_t converged, pad_;
     double rnorm, rr0, rr, beta, final_res;
-    double rzp[2];  // r.z of the current inner iteration, alternating by iteration parity
+    double rzp[2];      // r.z of the current inner iteration, alternating by iteration parity
+    double rnorm_prev;  // scale of the previous inner solve
+    double rz_keep;     // r.z of the last completed iteration of the previous inner solve
+    double gamma;       // p = z + gamma p at an inner start (0: fresh start)
 };
 
 struct SysRef {
@@ -240,6 +247,7 @@ __global__ void __launch_bounds__(kScalarThreads)
             if (threadIdx.x == 0) {
                 const double rnorm = sqrt(rr);
                 const double res = rnorm / S.bnorm;
+                S.rnorm_prev = S.rnorm;
                 S.rnorm = rnorm;
                 S.final_res = res;
                 if (res < S.tol) {
@@ -255,6 +263,20 @@ __global__ void __launch_bounds__(kScalarThreads)
         } else {  // kStart
             const double2 t = ordered_sum_all<true>(part_tile, ref.tile0, ref.tile1, red);
             if (threadIdx.x == 0) {
+                // Reliable update: after the first inner solve the Krylov
+                // direction is kept -- the true residual replaces the recurred
+                // one and the CG step continues with p = z + gamma p, gamma =
+                // beta of unscaled CG times the scale change (s_new / s_old):
+                // (s_new / s_old) (r.z)_new / (r.z)_last.  Only while the
+                // recurrence still tracks the true residual (the new |b - Ax|
+                // within 2x of the inner solve's estimate rnorm_prev |r|);
+                // when it does not (low-precision values, ill conditioning)
+                // the inner solve restarts from p = z.
+                const double est = S.rnorm_prev * sqrt(S.rr);
+                const bool cont = S.outer >= 2 && S.rz_keep > 0.0 && S.rnorm_prev > 0.0 &&
+                                  t.x > 0.0 && est > 0.0 && S.rnorm <= 2.0 * est &&
+                                  S.rnorm >= 0.5 * est;
+                S.gamma = cont ? (S.rnorm / S.rnorm_prev) * (t.x / S.rz_keep) : 0.0;
                 S.rzp[0] = t.x;
                 S.rzp[1] = t.x;
                 S.rr0 = t.y > 0.0 ? t.y : 1.0;
@@ -328,12 +350,13 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// Start an inner solve: r = r64 / rnorm, z = M^-1 r, p = z, d = 0; partials (r.z, r.r).
+// Start an inner solve: r = r64 / rnorm, z = M^-1 r, d = 0; partials (r.z,
+// r.r).  p is set by bs_pstart once r.z is known.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
     bs_inner_start(const int4* tiles, const int32_t* count, const SysState* sys,
                    const double* __restrict__ r64, const T* __restrict__ dinv, T* __restrict__ r,
-                   T* __restrict__ z, T* __restrict__ p, T* __restrict__ d, double* part) {
+                   T* __restrict__ z, T* __restrict__ d, double* part) {
     __shared__ double2 red[kWarps + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
@@ -347,7 +370,6 @@ __global__ void __launch_bounds__(kThreads)
                 const T zi = dinv[row] * ri;
                 r[row] = ri;
                 z[row] = zi;
-                p[row] = zi;
                 d[row] = T(0);
                 rz += ri * zi;
                 rr += ri * ri;
@@ -355,6 +377,27 @@ __global__ void __launch_bounds__(kThreads)
         }
         const double2 t = block_sum2_all(double(rz), double(rr), red);
         if (threadIdx.x == 0) reinterpret_cast<double2*>(part)[i] = t;
+    }
+}
+
+// Inner start, second half: p = z (fresh start) or p = z + gamma p (continued
+// Krylov direction), for the systems the start just moved to the inner phase.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    bs_pstart(const int4* tiles, const int32_t* count, const SysState* sys,
+              const T* __restrict__ z, T* __restrict__ p) {
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int4 tl = tiles[i];
+        if (sys_phase(sys, tl.z) != kSysInner) continue;
+        const double g = __ldcg(&sys[tl.z].gamma);
+        if (g == 0.0) {
+            for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x) p[row] = z[row];
+        } else {
+            const T gt = T(g);
+            for (int32_t row = tl.x + threadIdx.x; row < tl.y; row += blockDim.x)
+                p[row] = fma(gt, p[row], z[row]);
+        }
     }
 }
 
@@ -468,14 +511,15 @@ __global__ void __launch_bounds__(kThreads)
                       !(est >= __ldcg(&S.stop_frac) * __ldcg(&S.tol)) ||
                       __ldcg(&S.it_total) >= __ldcg(&S.max_iter);
     const bool first = i == tr.x;
+    const double rz_old = __ldcg(&S.rzp[par]);
     if (stop) {  // stop the inner solve; refine next step
         if (first && threadIdx.x == 0) {
             sys[slot].rr = t.y;
+            sys[slot].rz_keep = rz_old;
             sys[slot].phase = kSysOuter;
         }
         return;
     }
-    const double rz_old = __ldcg(&S.rzp[par]);
     const double beta_d = t.x / rz_old;
     const T beta = T(beta_d);
 #pragma unroll
@@ -595,7 +639,11 @@ struct nm_solver {
     unsigned char* stage = nullptr;
     size_t stage_cap = 0, stage_used = 0;
     unsigned int* err = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // the iterations
+    cudaStream_t up = nullptr;      // admission uploads (overlap a running step)
+    cudaEvent_t up_ev = nullptr;    // orders the uploads before the next kernels
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // device time of the running step
+    bool in_step = false;           // between nm_solver_step_begin and _end
     nm_solver_counters ctr{};
     ~nm_solver();
 };
@@ -612,6 +660,10 @@ nm_solver::~nm_solver() {
     cudaFreeHost(h_sblk); cudaFreeHost(h_stile);
     cudaFreeHost(h_blk); cudaFreeHost(h_tile); cudaFreeHost(h_ref); cudaFreeHost(stage);
     if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    if (up_ev) cudaEventDestroy(up_ev);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (up) cudaStreamDestroy(up);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -710,13 +762,13 @@ int upload_lists(nm_solver* S) {
     return NM_OK;
 }
 
-// `bytes` of pinned staging for an asynchronous upload on S->stream.  When
-// the staging buffer is full the stream is drained first (its earlier uploads
-// are then complete) and the buffer reused or grown.
+// `bytes` of pinned staging for an asynchronous upload on S->up.  When the
+// staging buffer is full the upload stream is drained first (its earlier
+// uploads are then complete) and the buffer reused or grown.
 int stage_alloc(nm_solver* S, size_t bytes, void** out) {
     bytes = (bytes + 255) & ~size_t(255);
     if (S->stage_used + bytes > S->stage_cap) {
-        NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+        NM_CUDA_TRY(cudaStreamSynchronize(S->up));
         S->stage_used = 0;
         if (bytes > S->stage_cap) {
             cudaFreeHost(S->stage);
@@ -800,10 +852,11 @@ int launch_outer(nm_solver* S) {
                                                            S->part_blk, S->part_tile);
     bs_inner_start<T><<<g_vec, kThreads, 0, s>>>(
         S->otile, &H->otile, S->st, S->r64, static_cast<const T*>(S->dinv),
-        static_cast<T*>(S->r), static_cast<T*>(S->z), static_cast<T*>(S->p),
-        static_cast<T*>(S->d), S->part_tile);
+        static_cast<T*>(S->r), static_cast<T*>(S->z), static_cast<T*>(S->d), S->part_tile);
     bs_scalar<kStart><<<g_sys, kScalarThreads, 0, s>>>(S->osys, &H->osys, S->st, S->part_blk,
                                                        S->part_tile);
+    bs_pstart<T><<<g_vec, kThreads, 0, s>>>(S->otile, &H->otile, S->st,
+                                            static_cast<const T*>(S->z), static_cast<T*>(S->p));
     NM_CHECK_LAUNCH();
     return NM_OK;
 }
@@ -815,6 +868,7 @@ int prepare_solver_kernels(nm_solver* S) {
     cudaFuncAttributes fa;
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_update<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pupdate<T>));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pstart<T>));
     int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
                             spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
     if (st != NM_OK) return st;
@@ -829,18 +883,21 @@ int prepare_solver_kernels(nm_solver* S) {
     return NM_OK;
 }
 
+// FP64 -> BF16 through FP32, round to nearest even, NaN kept quiet; written
+// without branches so the loop vectorises.
 void to_bf16(const double* v, size_t n, uint16_t* out) {
     for (size_t i = 0; i < n; ++i) {
         const float f = static_cast<float>(v[i]);
         uint32_t u;
         std::memcpy(&u, &f, 4);
-        if ((u & 0x7fffffffu) > 0x7f800000u) {
-            out[i] = static_cast<uint16_t>((u >> 16) | 0x40u);  // quiet NaN
-        } else {
-            u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even
-            out[i] = static_cast<uint16_t>(u >> 16);
-        }
+        const uint32_t rounded = (u + 0x7fffu + ((u >> 16) & 1u)) >> 16;
+        const uint32_t quiet = (u >> 16) | 0x40u;
+        out[i] = static_cast<uint16_t>((u & 0x7fffffffu) > 0x7f800000u ? quiet : rounded);
     }
+}
+
+void to_f32(const double* v, size_t n, float* out) {
+    for (size_t i = 0; i < n; ++i) out[i] = static_cast<float>(v[i]);
 }
 
 }  // namespace
@@ -903,9 +960,22 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     }
     NM_CUDA_TRY(cudaMallocHost(&S->h_sblk, sizeof(int2) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMallocHost(&S->h_stile, sizeof(int2) * size_t(max_systems)));
-    int st = grow_lists(S.get(), 1024, 1024);
+    // Lists sized for a full arena of typical systems (they still grow if a
+    // workload needs more): one descriptor per kSolverTile/2 nonzeros or per
+    // 128 rows, two per system; one tile per kTileRows rows, two per system.
+    const int64_t blk0 = std::max(max_nnz / (kSolverTile / 2), max_rows / 128) + 2 * max_systems;
+    const int64_t tile0 = max_rows / kTileRows + 2 * int64_t(max_systems);
+    int st = grow_lists(S.get(), blk0, tile0);
     if (st != NM_OK) return st;
+    // Pinned staging of admissions, allocated once (grows only for a single
+    // system larger than it).
+    S->stage_cap = size_t(256) << 20;
+    NM_CUDA_TRY(cudaMallocHost(&S->stage, S->stage_cap));
     NM_CUDA_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    NM_CUDA_TRY(cudaStreamCreateWithFlags(&S->up, cudaStreamNonBlocking));
+    NM_CUDA_TRY(cudaEventCreateWithFlags(&S->up_ev, cudaEventDisableTiming));
+    NM_CUDA_TRY(cudaEventCreate(&S->ev0));
+    NM_CUDA_TRY(cudaEventCreate(&S->ev1));
     S->err = device_error_word();
     if (!S->err) return fail(NM_ERR_CUDA, "nm_solver_create: cannot map the device error word");
     switch (S->inner) {
@@ -920,7 +990,10 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
 
 extern "C" int nm_solver_destroy(nm_solver* S) {
     nm::clear_error();
-    if (S) cudaStreamSynchronize(S->stream);
+    if (S) {
+        cudaStreamSynchronize(S->stream);
+        cudaStreamSynchronize(S->up);
+    }
     delete S;
     return NM_OK;
 }
@@ -1074,8 +1147,6 @@ void job_prep(const nm_solver* S, AdmitJob& J, bool inner_threads) {
                 const int32_t c = ci[j];
                 if ((c < 0 || c >= n) && badc < 0) badc = c;
                 gci[j] = r0 + c;
-                v64s[j] = val[j];
-                if (inner == NM_F32) static_cast<float*>(vins)[j] = static_cast<float>(val[j]);
                 if (c == i) dg += val[j];
             }
             const double di = (precond && dg != 0.0) ? 1.0 / dg : 1.0;
@@ -1084,8 +1155,12 @@ void job_prep(const nm_solver* S, AdmitJob& J, bool inner_threads) {
             bs[i] = J.b[i];
             if (J.x0) x0s[i] = J.x0[i];
         }
-        if (inner == NM_BF16 && i1 > i0)
-            to_bf16(val + rp[i0], size_t(rp[i1] - rp[i0]), static_cast<uint16_t*>(vins) + rp[i0]);
+        if (i1 > i0) {
+            const size_t z0c = size_t(rp[i0]), nzc = size_t(rp[i1] - rp[i0]);
+            std::memcpy(v64s + z0c, val + z0c, sizeof(double) * nzc);
+            if (inner == NM_F32) to_f32(val + z0c, nzc, static_cast<float*>(vins) + z0c);
+            if (inner == NM_BF16) to_bf16(val + z0c, nzc, static_cast<uint16_t*>(vins) + z0c);
+        }
         std::lock_guard<std::mutex> g(mu);
         if (badc >= 0 && J.bad_col < 0) J.bad_col = badc;
     };
@@ -1151,7 +1226,7 @@ int job_commit(nm_solver* S, AdmitJob& J) {
     }
     const size_t n = size_t(J.n), nz = size_t(J.row_ptr[J.n]);
     const size_t tb = inner_bytes(S->inner), vb = inner_val_bytes(S->inner);
-    cudaStream_t s = S->stream;
+    cudaStream_t s = S->up;
     const int64_t r0 = J.r0, z0 = J.z0;
     NM_CUDA_TRY(cudaMemcpyAsync(S->rp + r0, ptr[0], sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s));
     if (nz) {
@@ -1192,8 +1267,9 @@ int job_commit(nm_solver* S, AdmitJob& J) {
 int admit_jobs(nm_solver* S, AdmitJob* jobs, int32_t count, int32_t* admitted) {
     *admitted = 0;
     int32_t done = 0;
-    // Sub-batches bounded by a staging budget so pinned staging stays modest.
-    constexpr size_t kBatchStage = size_t(512) << 20;
+    // Sub-batches of at most half the staging buffer, so they fit it without
+    // growing it.
+    const size_t kBatchStage = std::max<size_t>(S->stage_cap / 2, size_t(1) << 20);
     while (done < count) {
         int32_t k = done;
         size_t bytes = 0;
@@ -1219,14 +1295,20 @@ int admit_jobs(nm_solver* S, AdmitJob* jobs, int32_t count, int32_t* admitted) {
             jobs[j].stage = base;
             base += stage_total(S, jobs[j]);
         }
-        const bool one = end - done == 1;
-        if (one) {
-            job_prep(S, jobs[done], true);
-        } else {
-            parallel_for(end - done, 1, [&](int64_t a, int64_t b) {
-                for (int64_t j = a; j < b; ++j) job_prep(S, jobs[done + j], false);
-            });
+        const auto tp = std::chrono::steady_clock::now();
+        // large systems one at a time, each over all host threads; the rest
+        // in parallel, one thread per system
+        constexpr int32_t kLargeRows = 65536;
+        std::vector<int32_t> small;
+        for (int32_t j = done; j < end; ++j) {
+            if (jobs[j].n >= kLargeRows || end - done == 1) job_prep(S, jobs[j], true);
+            else small.push_back(j);
         }
+        parallel_for(int64_t(small.size()), 1, [&](int64_t a, int64_t b) {
+            for (int64_t j = a; j < b; ++j) job_prep(S, jobs[small[size_t(j)]], false);
+        });
+        const auto tc = std::chrono::steady_clock::now();
+        S->ctr.s_admit_prep += std::chrono::duration<double>(tc - tp).count();
         for (int32_t j = done; j < end; ++j) {
             if (jobs[j].bad_col >= 0 || jobs[j].bad_rp) {
                 const AdmitJob& b = jobs[j];
@@ -1241,6 +1323,8 @@ int admit_jobs(nm_solver* S, AdmitJob* jobs, int32_t count, int32_t* admitted) {
             if (cst != NM_OK) return cst;
             ++*admitted;
         }
+        S->ctr.s_admit_commit +=
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - tc).count();
         done = end;
         if (st != NM_OK) return st;  // stopped early (no room or an invalid system)
     }
@@ -1286,12 +1370,13 @@ extern "C" int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t*
     return st;
 }
 
-extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
+extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
     using namespace nm;
     using clk = std::chrono::steady_clock;
     clear_error();
-    if (!S) return fail(NM_ERR_INVALID, "nm_solver_step: NULL solver");
-    if (iters < 0) return fail(NM_ERR_INVALID, "nm_solver_step: iters must be >= 0");
+    if (!S) return fail(NM_ERR_INVALID, "nm_solver_step_begin: NULL solver");
+    if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_step_begin: a step is running");
+    if (iters < 0) return fail(NM_ERR_INVALID, "nm_solver_step_begin: iters must be >= 0");
     iters = (iters + 1) & ~1;  // whole pairs (the r.z double buffer alternates)
     int st = NM_OK;
     auto t0 = clk::now();
@@ -1300,15 +1385,20 @@ extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
         acc += std::chrono::duration<double>(t - t0).count();
         t0 = t;
     };
+    // admissions' uploads land before anything reads the new systems
+    NM_CUDA_TRY(cudaEventRecord(S->up_ev, S->up));
+    NM_CUDA_TRY(cudaStreamWaitEvent(S->stream, S->up_ev, 0));
     if (S->lists_dirty) {
         st = upload_lists(S);
         if (st != NM_OK) return st;
         S->ctr.list_uploads += 1;
     }
     lap(S->ctr.s_lists);
+    S->in_step = true;
+    NM_CUDA_TRY(cudaEventRecord(S->ev0, S->stream));
     const ListHdr& H = *S->h_hdr;
     if (H.isys == 0) {
-        if (n_done) *n_done = 0;
+        NM_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
         return NM_OK;
     }
     S->ctr.steps += 1;
@@ -1362,12 +1452,33 @@ extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
         NM_CUDA_TRY(cudaGraphLaunch(S->chunk_exec, S->stream));
         S->ctr.inner_iterations += iters;
     }
+    NM_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
+    return NM_OK;
+}
+
+extern "C" int nm_solver_step_end(nm_solver* S, int32_t* n_done) {
+    using namespace nm;
+    using clk = std::chrono::steady_clock;
+    clear_error();
+    if (!S) return fail(NM_ERR_INVALID, "nm_solver_step_end: NULL solver");
+    if (!S->in_step) return fail(NM_ERR_INVALID, "nm_solver_step_end: no step is running");
+    S->in_step = false;
+    auto t0 = clk::now();
+    // uploads of systems admitted during the step land before the state read-back
+    NM_CUDA_TRY(cudaEventRecord(S->up_ev, S->up));
+    NM_CUDA_TRY(cudaStreamWaitEvent(S->stream, S->up_ev, 0));
     NM_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(SysState) * size_t(S->cap_sys),
                                 cudaMemcpyDeviceToHost, S->stream));
     NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
-    lap(S->ctr.s_run);
     S->stage_used = 0;  // every staged upload has landed
-    st = nm_check_device_errors();
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) {
+        S->ctr.last_step_ms = ms;
+        S->ctr.s_device += ms * 1e-3;
+    }
+    S->ctr.s_run += std::chrono::duration<double>(clk::now() - t0).count();
+    t0 = clk::now();
+    int st = nm_check_device_errors();
     if (st != NM_OK) return st;
     int32_t done = 0;
     for (int32_t k = 0; k < S->cap_sys; ++k) {
@@ -1382,8 +1493,21 @@ extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
         }
     }
     if (n_done) *n_done = done;
-    lap(S->ctr.s_scan);
+    S->ctr.s_scan += std::chrono::duration<double>(clk::now() - t0).count();
     return NM_OK;
+}
+
+extern "C" int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done) {
+    const int st = nm_solver_step_begin(S, iters);
+    if (st != NM_OK) {
+        if (S && S->in_step) {  // end the step without hiding the first error
+            const std::string msg = nm_last_error();
+            nm_solver_step_end(S, nullptr);
+            return fail(st, "%s", msg.c_str());
+        }
+        return st;
+    }
+    return nm_solver_step_end(S, n_done);
 }
 
 extern "C" int nm_solver_counters_get(const nm_solver* S, nm_solver_counters* out) {
@@ -1415,6 +1539,7 @@ extern "C" int nm_solver_take(nm_solver* S, int32_t slot, double* x_host) {
     clear_error();
     if (!S || slot < 0 || slot >= S->cap_sys || !S->sys[slot].used)
         return fail(NM_ERR_INVALID, "nm_solver_take: no system in slot %d", slot);
+    if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_take: a step is running");
     HostSys& h = S->sys[slot];
     if (x_host)
         NM_CUDA_TRY(cudaMemcpyAsync(x_host, S->x + h.row0, sizeof(double) * size_t(h.n),

@@ -2,11 +2,12 @@
 plain FP64 CG drop-in run one request at a time for comparison.
 
 A request is (arrival time in seconds, A, b).  `serve` runs a real-time loop:
-requests that have arrived are admitted in arrival order while the arena has
-room for them (admission by free device memory), every loop iteration runs one
-engine step (pending refinement steps + `chunk` lockstep iterations of all live
-solves), finished solves are retired and their latency (finish - arrival)
-recorded.  `serve_plain` solves the same requests one at a time, in arrival
+every loop iteration starts one engine step (pending refinement steps + `chunk`
+lockstep iterations of all live solves) and, while the device runs it, admits
+the requests that have arrived, in arrival order, while the arena has room for
+them (admission by free device memory; they join at the next step); then it
+waits for the step, retires finished solves and records their latency (finish
+- arrival).  `serve_plain` solves the same requests one at a time, in arrival
 order, with the drop-in FP64 CG (`kokkos_spmv.cg_solve_local` semantics: upload,
 solve, copy back).
 """
@@ -58,30 +59,71 @@ def _stats(lat, t0, t_end, n_done):
 
 
 def serve(requests, solver, tol: float = 1e-8, max_iter: int = 100000, chunk: int = 8,
-          check=None):
-    """Continuous batching.  Returns (stats, per-request records)."""
+          check=None, batch: int = 16):
+    """Continuous batching.  Returns (stats, per-request records).  `batch`:
+    requests prepared per admission call (in parallel on the host)."""
     order = sorted(range(len(requests)), key=lambda i: requests[i][0])
     queue = []  # arrived, not yet admitted (FIFO)
     nxt = 0
     live = {}   # slot -> request index
     rec = [None] * len(requests)
     t0 = time.perf_counter()
-    while nxt < len(order) or queue or live:
+    def arrivals():
+        nonlocal nxt
         now = time.perf_counter() - t0
         while nxt < len(order) and requests[order[nxt]][0] <= now:
             queue.append(order[nxt])
             nxt += 1
-        if queue:
-            got = solver.admit_many([requests[i][1:3] for i in queue[:256]], tol=tol,
-                                    max_iter=max_iter)
-            for slot, i in zip(got, queue):
-                live[slot] = i
-            del queue[: len(got)]
+
+    def admit(count):
+        got = solver.admit_many([requests[i][1:3] for i in queue[:count]], tol=tol,
+                                max_iter=max_iter)
+        for slot, i in zip(got, queue):
+            live[slot] = i
+        del queue[: len(got)]
+        return len(got) == min(count, len(queue) + len(got))  # False: no room
+
+    def admit_budgeted(budget):
+        # admit in small batches while the device is still busy with the step
+        t_start = time.perf_counter()
+        while queue and time.perf_counter() - t_start < budget:
+            if not admit(batch):
+                break
+            arrivals()
+
+    def step_iters():
+        # While requests wait, size the step so that its device time covers
+        # the host time of admitting the next batch (both estimated from the
+        # counters: device ms per iteration of the last step, host seconds of
+        # preparation per admitted row so far).
+        if not queue:
+            return chunk, 0.0
+        c = solver.counters()
+        rows_done = max(1, solver.rows_admitted)
+        per_row = c["s_admit_prep"] / rows_done if c["s_admit_prep"] > 0 else 1e-7
+        nxt_rows = sum(requests[i][1].nrows for i in queue[:batch])
+        need = per_row * nxt_rows
+        last = c["last_step_ms"] * 1e-3
+        per_it = last / max(1, solver.last_iters) if last > 0 else 0.0
+        if per_it <= 0:
+            return chunk * 4, need
+        it = int(min(64 * chunk, max(chunk, need / per_it)))
+        return it, need
+
+    while nxt < len(order) or queue or live:
+        arrivals()
         if not live:
-            if nxt < len(order):  # idle until the next arrival
-                time.sleep(max(0.0, requests[order[nxt]][0] - (time.perf_counter() - t0)))
-            continue
-        for slot in solver.step(chunk):
+            if queue:
+                admit(batch)  # a first batch to start the device
+            if not live:
+                if nxt < len(order):  # idle until the next arrival
+                    time.sleep(max(0.0, requests[order[nxt]][0] - (time.perf_counter() - t0)))
+                continue
+        iters, budget = step_iters()
+        solver.step_begin(iters)
+        arrivals()
+        admit_budgeted(max(budget, 1e-3))  # host preparation overlaps the step on the device
+        for slot in solver.step_end():
             i = live.pop(slot)
             x, info = solver.take(slot)
             t_fin = time.perf_counter() - t0

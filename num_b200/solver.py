@@ -62,6 +62,8 @@ class BatchSolver:
         self.n = {}          # slot -> rows
         self.active = set()  # slots not yet finished
         self.seconds = {"admit": 0.0, "step": 0.0, "take": 0.0}  # host wall time per call kind
+        self.rows_admitted = 0  # rows of all systems admitted so far
+        self.last_iters = 0     # inner iterations of the last step (rounded up to even)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -97,6 +99,7 @@ class BatchSolver:
         _lib.check(st, "admit")
         self.n[slot.value] = int(n)
         self.active.add(slot.value)
+        self.rows_admitted += int(n)
         return slot.value
 
     def admit_many(self, systems, tol: float = 1e-8, max_iter: int = 10000):
@@ -130,15 +133,29 @@ class BatchSolver:
         for i, s in enumerate(out):
             self.n[s] = int(ns[i])
             self.active.add(s)
+            self.rows_admitted += int(ns[i])
         _lib.check(st, "admit_many")
         return out
 
     def step(self, iters: int = 8):
-        """Refinement steps + `iters` inner iterations; returns the slots that
-        finished in this step."""
+        """Refinement steps + `iters` inner iterations (rounded up to even);
+        returns the slots that finished in this step."""
+        self.step_begin(iters)
+        return self.step_end()
+
+    def step_begin(self, iters: int = 8):
+        """Enqueue a step and return at once; admit() / admit_many() may run
+        before step_end() (their host work overlaps the device)."""
+        t0 = time.perf_counter()
+        _lib.check(self.lib.nm_solver_step_begin(self._h, int(iters)), "step")
+        self.last_iters = (int(iters) + 1) & ~1
+        self.seconds["step"] += time.perf_counter() - t0
+
+    def step_end(self):
+        """Wait for the step; returns the slots that finished in it."""
         nd = C.c_int32(0)
         t0 = time.perf_counter()
-        _lib.check(self.lib.nm_solver_step(self._h, int(iters), C.byref(nd)), "step")
+        _lib.check(self.lib.nm_solver_step_end(self._h, C.byref(nd)), "step")
         self.seconds["step"] += time.perf_counter() - t0
         done = []
         if nd.value:
@@ -188,14 +205,22 @@ class BatchSolver:
         out = [None] * len(systems)
         owner = {}
         nxt = 0
+
+        def admit():
+            nonlocal nxt
+            got = self.admit_many(systems[nxt:nxt + 1024], tol=tol, max_iter=max_iter)
+            for s in got:
+                owner[s] = nxt
+                nxt += 1
+            return got
+
         while nxt < len(systems) or self.active:
-            if nxt < len(systems):
-                got = self.admit_many(systems[nxt:nxt + 1024], tol=tol, max_iter=max_iter)
-                if not got and not self.active:
+            if not self.active:
+                if not admit():
                     raise MemoryError("solve: a system does not fit the empty arena")
-                for s in got:
-                    owner[s] = nxt
-                    nxt += 1
-            for s in self.step(chunk):
+            self.step_begin(chunk)
+            if nxt < len(systems):
+                admit()  # host preparation overlaps the step
+            for s in self.step_end():
                 out[owner.pop(s)] = self.take(s)
         return out
