@@ -6,13 +6,32 @@ Default workload (one step = one FP64 CSR SpMV, y = A x):
   int32 indices, FP64 values, x ~ U[-1, 1] (default_rng(1)).
   Algorithmic bytes per SpMV = 12 nnz + 4 (n + 1) + 8 n (x) + 8 n (y)
   = 424.14 MB, larger than the 126 MB L2, so no flush is needed between steps.
+  The default line also carries a `secondary` object: plain FP64 CG solves/s
+  on the 256^2 Laplacian and a served-CG sample (see serve_c5).
+
+Other workloads (--workload):
+  spmv_c2a_fp32, spmv_c2b[_fp32], spmv_c1     one SpMV per step
+  spmv_c3[_fp32]    4,096 banded SPD matrices (n log-uniform in [32, 4096],
+                    seed 2) multiplied in one launch per step
+  cg_c1             one plain FP64 CG solve per step (256^2 Laplacian,
+                    b = A 1, x0 = 0, tol 1e-8), the drop-in cg_solve_local
+  cg_c4_fp64 / cg_c4_fp32 / cg_c4_bf16
+                    one Jacobi-PCG solve per step of the 128^3 variable-
+                    coefficient Poisson system (seed 3) to 1e-10 through the
+                    batched engine: FP64, or FP32 / BF16 values with FP64
+                    iterative refinement
+  serve_c5          one pass of a served request stream per step (Poisson
+                    arrivals, seed 4; Laplacians and banded SPD systems),
+                    FP32 inner + FP64 refinement, tol 1e-8, continuous
+                    batching; compared with the plain FP64 drop-in run one
+                    request at a time
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
     python bench.py --impl reference ...   # the reference's CPU path (oracle port)
 
 Multi-GPU (torchrun, one rank per GPU): every rank runs the same workload on
 its own GPU (independent replicas, weak scaling, no data-path collective);
-value = total bytes of all ranks / max-over-ranks time.
+value = total work of all ranks / max-over-ranks time.
 Prints one JSON line on rank 0.
 """
 from __future__ import annotations
@@ -34,12 +53,29 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "CG solves/s + p99 latency at rel-res 1e-8 vs plain FP64 CG; SpMV HBM GB/s"
 
+# name -> (description, kind, precision)
 WORKLOADS = {
-    "spmv_c2a": ("3-D 7-point Laplacian 160^3, FP64 CSR SpMV", "fp64"),
-    "spmv_c2a_fp32": ("3-D 7-point Laplacian 160^3, FP32 CSR SpMV", "fp32"),
-    "spmv_c2b": ("power-law rows n=2,000,000 mean 16 sigma 1.2, FP64 CSR SpMV", "fp64"),
-    "spmv_c2b_fp32": ("power-law rows n=2,000,000 mean 16 sigma 1.2, FP32 CSR SpMV", "fp32"),
-    "spmv_c1": ("2-D 5-point Laplacian 256^2, FP64 CSR SpMV", "fp64"),
+    "spmv_c2a": ("3-D 7-point Laplacian 160^3, FP64 CSR SpMV", "spmv", "fp64"),
+    "spmv_c2a_fp32": ("3-D 7-point Laplacian 160^3, FP32 CSR SpMV", "spmv", "fp32"),
+    "spmv_c2b": ("power-law rows n=2,000,000 mean 16 sigma 1.2, FP64 CSR SpMV", "spmv", "fp64"),
+    "spmv_c2b_fp32": ("power-law rows n=2,000,000 mean 16 sigma 1.2, FP32 CSR SpMV", "spmv",
+                      "fp32"),
+    "spmv_c1": ("2-D 5-point Laplacian 256^2, FP64 CSR SpMV", "spmv", "fp64"),
+    "spmv_c3": ("4,096 banded SPD matrices n log-U[32,4096] (seed 2), FP64 SpMV of all in one "
+                "launch", "spmv", "fp64"),
+    "spmv_c3_fp32": ("4,096 banded SPD matrices n log-U[32,4096] (seed 2), FP32 SpMV of all in "
+                     "one launch", "spmv", "fp32"),
+    "cg_c1": ("2-D 5-point Laplacian 256^2, plain FP64 CG, b = A*1, x0 = 0, tol 1e-8", "cg",
+              "fp64"),
+    "cg_c4_fp64": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG FP64 to 1e-10",
+                   "engine", "fp64"),
+    "cg_c4_fp32": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG FP32 + FP64 "
+                   "iterative refinement to 1e-10", "engine", "fp32"),
+    "cg_c4_bf16": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG BF16 values + "
+                   "FP64 iterative refinement to 1e-10", "engine", "bf16"),
+    "serve_c5": ("served CG stream (seed 4): 50/50 2-D Laplacian side log-U[32,1024] or banded "
+                 "SPD n log-U[256,65536], b ~ N(0,1), Jacobi PCG to 1e-8, FP32 inner + FP64 "
+                 "refinement, continuous batching", "serve", "fp32"),
 }
 
 
@@ -51,13 +87,32 @@ def make_workload(name):
     elif name.startswith("spmv_c2b"):
         A = gen.power_law(2_000_000, seed=1001)
         seed = 1
-    elif name == "spmv_c1":
+    elif name in ("spmv_c1", "cg_c1"):
         A = gen.laplacian_2d(256)
         seed = 0
+    elif name.startswith("spmv_c3"):
+        mats, xs = gen.banded_batch(4096, seed=2)
+        return mats, np.concatenate(xs)
     else:
         raise SystemExit(f"unknown workload {name}")
     x = np.random.default_rng(seed).uniform(-1.0, 1.0, A.ncols)
     return A, x
+
+
+def block_diagonal(mats):
+    """One host CSR holding the matrices on the diagonal (for byte counts and
+    the CPU legs)."""
+    from num_b200.generators import Csr
+    rps, cis, vals = [np.zeros(1, np.int64)], [], []
+    r = z = 0
+    for A in mats:
+        rps.append(A.row_ptr[1:].astype(np.int64) + z)
+        cis.append(A.col_idx.astype(np.int64) + r)
+        vals.append(A.values)
+        r += A.nrows
+        z += A.nnz
+    return Csr(np.concatenate(rps).astype(np.int32), np.concatenate(cis).astype(np.int32),
+               np.concatenate(vals), r, r)
 
 
 def spmv_bytes(A, precision):
@@ -65,6 +120,31 @@ def spmv_bytes(A, precision):
     vb = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
     xb = 8 if precision == "fp64" else 4
     return sb(A.nnz, A.nrows, A.ncols, vb, xb)
+
+
+def cg_iter_bytes(nnz, n, vb, tb):
+    """Algorithmic bytes of one CG iteration as the library runs it (three
+    kernels): SpMV with p.Ap (values + int32 columns + row_ptr, the gathered
+    p once, Ap written), the x/r update with r.r (x, p, r, Ap read; x, r
+    written) and the p update (r, p read; p written) -- 11 vector passes of
+    tb bytes.  With a Jacobi preconditioner (the engine) the update also reads
+    the inverse diagonal and the correction d and writes z: 13 passes."""
+    return (vb + 4) * nnz + 4 * (n + 1) + 11 * tb * n
+
+
+def engine_iter_bytes(nnz, n, vb, tb):
+    """One inner iteration of the batched engine: SpMV with p.Ap (values +
+    columns + row_ptr, p gathered once, Ap written); update (p, Ap, r, d,
+    D^-1 read; d, r, z written); p update (z, p read; p written)."""
+    return (vb + 4) * nnz + 4 * (n + 1) + 13 * tb * n
+
+
+def engine_outer_bytes(nnz, n, tb):
+    """One refinement step: x += s d (d, x read, x written: 16 + tb), the FP64
+    residual SpMV (values, columns, row_ptr; x gathered, b read, r64 written:
+    24), the inner start (r64, D^-1 read; r, z, d written: 8 + 4 tb) and
+    p = z + g p (z, p read, p written: 3 tb)."""
+    return 12 * nnz + 4 * (n + 1) + (48 + 8 * tb) * n
 
 
 def measured_peak():
@@ -156,20 +236,55 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-# ---- our arm ---------------------------------------------------------------------------
+def dtype_name(precision):
+    return {"fp64": "f64", "fp32": "f32", "bf16": "bf16/f32"}[precision]
 
-def run_ours(args, rank, world, local_rank):
+
+def max_over_ranks(values, world, dev):
+    if world == 1:
+        return [float(v) for v in values]
     import torch
     import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def base_line(args, world, value, unit, ms_per_step, precision, config, higher=True):
+    return {
+        "metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 6), "higher_is_better": higher,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_name(precision),
+        "data": "synthetic", "config": config,
+    }
+
+
+# ---- our arm: SpMV ---------------------------------------------------------------------
+
+def run_spmv(args, rank, world, local_rank):
+    import torch
 
     from num_b200 import _lib
     from num_b200 import kokkos_spmv as kspmv
 
-    kspmv.init(local_rank)
     dev = torch.device("cuda", local_rank)
-    desc, precision = WORKLOADS[args.workload]
+    desc, _, precision = WORKLOADS[args.workload]
     A, x = make_workload(args.workload)
-    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols, precision=precision)
+    if isinstance(A, list):  # many matrices, one launch
+        mats = A
+        M = kspmv.upload_csr_batched([m.astuple() for m in mats], precision=precision)
+        A = block_diagonal(mats)
+        batch = {"matrices": len(mats), "api": "upload_csr_batched"}
+    else:
+        M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols,
+                             precision=precision)
+        batch = None
     tuned = kspmv.tune(M, tile=args.tile, short_max=args.short_max, stages=args.stages,
                        grid_mult=args.grid_mult)
     dt = torch.float64 if precision == "fp64" else torch.float32
@@ -185,11 +300,13 @@ def run_ours(args, rank, world, local_rank):
         if st:
             _lib.check(st, "nm_spmv")
 
+    # Operands smaller than L2: flush it between steps (a 256 MB write, outside
+    # the per-step events) and time the steps alone.
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if nbytes < 126e6 else None
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -197,25 +314,21 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         t0.record(stream)
         for k in range(args.steps):
+            if flush is not None:
+                flush.zero_()
             ev[k][0].record(stream)
             step()
             ev[k][1].record(stream)
         t1.record(stream)
         torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     total_ms = t0.elapsed_time(t1)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
+    if flush is not None:
+        total_ms = sum(kern_ms)
     kern_avg_ms = sum(kern_ms) / len(kern_ms)
-    t = torch.tensor([total_ms, kern_avg_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, kern_avg_ms = float(t[0]), float(t[1])
+    total_ms, kern_avg_ms = max_over_ranks([total_ms, kern_avg_ms], world, dev)
     ms_per_step = total_ms / args.steps
-
-    # correctness spot check (outside the timed region)
-    if rank == 0 and args.workload == "spmv_c1":
-        pass
 
     # e2e through the public drop-in API: pinned host x -> device, spmv, y -> pinned host
     e2e_steps = max(3, min(args.steps, 50))
@@ -235,38 +348,26 @@ def run_ours(args, rank, world, local_rank):
         stream.synchronize()
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te[0])
+    e2e_ms = max_over_ranks([e0.elapsed_time(e1) / e2e_steps], world, dev)[0]
 
     if rank != 0:
         return None
     peak, peak_src = measured_peak()
     achieved = nbytes / (kern_avg_ms * 1e-3) / 1e9
-    line = {
-        "metric": METRIC,
-        "value": round(world * nbytes / (ms_per_step * 1e-3) / 1e9, 2),
-        "unit": "GB/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 6),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f64" if precision == "fp64" else ("f32" if precision == "fp32" else "bf16/f32"),
-        "data": "synthetic",
-        "config": {
-            "workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
-            "index": "int32", "values": precision,
-            "bytes_per_step": nbytes,
-            "bytes_formula": "12*nnz + 4*(n+1) + 8*ncols + 8*nrows (fp64)",
-            "l2": "inputs larger than L2 (no flush): %.1f MB per step > 126 MB" % (nbytes / 1e6),
-            "parallelism": f"replicas x{world}",
-            "tuning": tuned,
-        },
+    config = {
+        "workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
+        "index": "int32", "values": precision, "bytes_per_step": nbytes,
+        "bytes_formula": "(value bytes + 4)*nnz + 4*(n+1) + x bytes*ncols + y bytes*nrows",
+        "l2": ("inputs larger than L2 (no flush): %.1f MB per step > 126 MB" % (nbytes / 1e6)
+               if flush is None else "inputs smaller than L2 (%.1f MB): L2 flushed (256 MB "
+               "write) between steps, steps timed alone" % (nbytes / 1e6)),
+        "parallelism": f"replicas x{world}", "tuning": tuned,
+    }
+    if batch:
+        config["batch"] = batch
+    line = base_line(args, world, round(world * nbytes / (ms_per_step * 1e-3) / 1e9, 2), "GB/s",
+                     ms_per_step, precision, config)
+    line.update({
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src,
@@ -285,14 +386,345 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "reference_metric_gbs": round(
-            (12 * A.nnz + 16 * A.nrows) / (kern_avg_ms * 1e-3) / 1e9, 1) if precision == "fp64" else None,
-    }
+            (12 * A.nnz + 16 * A.nrows) / (kern_avg_ms * 1e-3) / 1e9, 1)
+        if precision == "fp64" else None,
+    })
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(A, x, precision, budget_s=args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline_spmv(A, x, precision, budget_s=args.cpu_seconds)
+    if world == 1 and args.workload == "spmv_c2a" and not args.no_secondary:
+        line["secondary"] = secondary(local_rank)
     return line
 
 
-# ---- CPU leg (oracle port of the reference's CPU path) --------------------------------------
+# ---- our arm: plain CG (the drop-in cg_solve_local) ------------------------------------
+
+def cg_c1_measure(dev, steps, warmup, with_clock=True, local_rank=0):
+    """Device-timed plain FP64 CG solves (b = A 1 resident, x zeroed on the
+    device each step) and the same through the public API with host copies."""
+    import torch
+
+    from num_b200 import kokkos_spmv as kspmv
+    A, _ = make_workload("cg_c1")
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    bh = A.to_scipy() @ np.ones(A.ncols)
+    b = torch.tensor(bh, device=dev)
+    x = torch.zeros(A.nrows, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        x.zero_()
+        info = kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=5000)
+    torch.cuda.synchronize(dev)
+    # the operands (11.5 MB) fit L2: flush it before every solve (outside the
+    # per-solve events)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    iters = 0
+    clk = ClockSampler(local_rank) if with_clock else None
+    if clk:
+        clk.__enter__()
+    for k in range(steps):
+        x.zero_()
+        flush.zero_()
+        ev[k][0].record(stream)
+        info = kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=5000)
+        ev[k][1].record(stream)
+        iters += info["iters"]
+    torch.cuda.synchronize(dev)
+    if clk:
+        clk.__exit__()
+    ms = sum(a.elapsed_time(c) for a, c in ev)
+    xs = x.cpu().numpy()
+    err = float(np.abs(xs - 1.0).max())
+    # e2e: pinned b in, x out, every solve
+    bp = torch.tensor(bh).pin_memory()
+    xp = torch.empty(A.nrows, dtype=torch.float64).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(3, min(steps, 20))
+    e0.record(stream)
+    for _ in range(e_steps):
+        b.copy_(bp, non_blocking=True)
+        x.zero_()
+        kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=5000)
+        xp.copy_(x, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = e0.elapsed_time(e1) / e_steps
+    return {"A": A, "ms": ms, "iters": iters, "info": info, "max_err_vs_ones": err,
+            "e2e_ms": e_ms, "h2d": bp.numel() * 8, "d2h": xp.numel() * 8,
+            "clocks": clk.summary() if clk else None}
+
+
+def run_cg(args, rank, world, local_rank):
+    import torch
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    barrier(world)
+    r = cg_c1_measure(dev, args.steps, args.warmup, local_rank=local_rank)
+    barrier(world)
+    ms, e2e_ms = max_over_ranks([r["ms"], r["e2e_ms"]], world, dev)
+    if rank != 0:
+        return None
+    A = r["A"]
+    it_per_solve = r["iters"] / args.steps
+    per_it = cg_iter_bytes(A.nnz, A.nrows, 8, 8)
+    peak, peak_src = measured_peak()
+    achieved = per_it * r["iters"] / (r["ms"] * 1e-3) / 1e9
+    ms_per = ms / args.steps
+    config = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
+              "tol": 1e-8, "iters_per_solve": it_per_solve,
+              "final_residual": r["info"]["residual"], "max_abs_err_vs_ones": r["max_err_vs_ones"],
+              "l2": "operands fit L2 (11.5 MB): L2 flushed before every solve, solves timed "
+                    "alone; within a solve the iterations are L2-resident and latency-bound",
+              "parallelism": f"replicas x{world}",
+              "api": "kokkos_spmv.cg_solve_local (C ABI nm_cg_local): 3 kernels per iteration "
+                     "in CUDA graph chunks"}
+    line = base_line(args, world, round(world * 1e3 / ms_per, 3), "solves/s", ms_per, precision,
+                     config)
+    line.update({
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                     "traffic": None, "kernel": "whole CG iteration (SpMV+p.Ap, x/r update, "
+                     "p update)", "bytes_per_iteration": per_it,
+                     "us_per_iteration": round(r["ms"] * 1e3 / r["iters"], 3)},
+        "e2e": {"value": round(1e3 / e2e_ms, 3), "unit": "solves/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                "ms_per_step": round(e2e_ms, 4),
+                "api": "kokkos_spmv.cg_solve_local with pinned b copied in and x copied out"},
+        "gpu_launches": int(r["iters"] * 3 + 2 * args.steps),
+        "clocks": r["clocks"],
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_cg(A, A.to_scipy() @ np.ones(A.ncols), 1e-8,
+                                               budget_s=args.cpu_seconds, precond=False)
+    return line
+
+
+# ---- our arm: the batched engine on one large system (C4) --------------------------------
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+
+    from num_b200 import generators as gen
+    from num_b200.solver import BatchSolver
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    A, b = gen.varcoef_poisson_3d(128, seed=3)
+    S = BatchSolver(A.nrows + 4096, A.nnz + 4096, 4, precision=precision)
+    slot = S.admit(A, b, tol=1e-10, max_iter=20000)
+    ext = torch.cuda.ExternalStream(S.stream(), device=dev)
+    chunk = 64
+
+    def solve_once():
+        S.resolve(slot)
+        while slot in S.active:
+            S.step(chunk)
+
+    while slot in S.active:  # the first solve (admission was outside)
+        S.step(chunk)
+    for _ in range(max(0, args.warmup - 1)):
+        solve_once()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    c0 = S.counters()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t0.record(ext)
+        for _ in range(args.steps):
+            solve_once()
+        t1.record(ext)
+        torch.cuda.synchronize(dev)
+    c1 = S.counters()
+    ms = t0.elapsed_time(t1)
+    st = S.status(slot)
+    x, _ = S.take(slot)
+    true_res = float(np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b))
+    # e2e: the whole public-API solve per step (admission from host arrays,
+    # steps, x copied back, slot freed)
+    e_steps = max(1, min(args.steps, 3))
+    e0 = time.perf_counter()
+    for _ in range(e_steps):
+        (xe, ie), = S.solve([(A, b)], tol=1e-10, max_iter=20000, chunk=chunk)
+    e_ms = (time.perf_counter() - e0) * 1e3 / e_steps
+    barrier(world)
+    ms, e_ms = max_over_ranks([ms, e_ms], world, dev)
+    if rank != 0:
+        return None
+    vb = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
+    tb = 8 if precision == "fp64" else 4
+    its = (c1["inner_iterations"] - c0["inner_iterations"]) / args.steps  # enqueued
+    outer = st["outer"]
+    per_solve = st["iters"] * engine_iter_bytes(A.nnz, A.nrows, vb, tb) + \
+        outer * engine_outer_bytes(A.nnz, A.nrows, tb)
+    peak, peak_src = measured_peak()
+    dev_s = (c1["s_device"] - c0["s_device"]) / args.steps
+    ms_per = ms / args.steps
+    achieved = per_solve / dev_s / 1e9 if dev_s > 0 else None
+    config = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
+              "tol": 1e-10, "inner_iterations": st["iters"], "outer_steps": outer,
+              "iterations_enqueued_per_solve": its, "residual": st["residual"],
+              "true_residual_fp64": true_res, "converged": st["converged"],
+              "chunk": chunk, "parallelism": f"replicas x{world}",
+              "api": "num_b200.solver.BatchSolver (C ABI nm_solver_*): admit once, "
+                     "nm_solver_resolve + steps per solve",
+              "l2": "inputs larger than L2 (%.0f MB of matrix values + indices)" %
+                    ((vb + 4) * A.nnz / 1e6)}
+    line = base_line(args, world, round(world * 1e3 / ms_per, 4), "solves/s", ms_per, precision,
+                     config)
+    line.update({
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None,
+                     "peak_source": peak_src, "traffic": None,
+                     "kernel": "whole engine iteration (SpMV+p.Ap, update, p update) + "
+                               "refinement steps, device time of the steps",
+                     "bytes_per_solve": per_solve},
+        "e2e": {"value": round(1e3 / e_ms, 4), "unit": "solves/s",
+                "h2d_bytes_per_step": int(A.nnz * (12 + vb) + A.nrows * 16),
+                "d2h_bytes_per_step": int(A.nrows * 8), "ms_per_step": round(e_ms, 3),
+                "api": "BatchSolver.solve: admission from host arrays, steps, take"},
+        "gpu_launches": int((c1["inner_iterations"] - c0["inner_iterations"]) * 3 +
+                            (c1["outer_launches"] - c0["outer_launches"]) * 6),
+        "clocks": clk.summary(),
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        # the CPU solves in FP64: scale to the FP64 Jacobi-PCG iteration count
+        # of this system (692, equal to the FP64 engine's)
+        line["cpu_baseline"] = cpu_baseline_cg(A, b, 1e-10, budget_s=args.cpu_seconds,
+                                               precond=True, full_iters=692)
+    return line
+
+
+# ---- our arm: served request stream (C5) -----------------------------------------------
+
+def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, local_rank=0):
+    """Served runs of the stream on one solver, and the plain drop-in once."""
+    import torch
+
+    from num_b200 import serve
+    from num_b200.solver import BatchSolver, arena_for
+    rows, nnz = arena_for(arena_bytes, nnz_per_row=5.0, precision="fp32")
+    S = BatchSolver(rows, nnz, 1024, precision="fp32")
+    ext = torch.cuda.ExternalStream(S.stream(), device=dev)
+    errs = []
+
+    def check_fn(i, x, info):
+        if len(errs) < 1000:
+            _, A, b, _ = requests[i]
+            errs.append(float(np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)))
+
+    for _ in range(warmup):
+        serve.serve(requests, S, tol=1e-8, chunk=16)
+    stats = []
+    c0 = S.counters()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local_rank)
+    with clk:
+        t0.record(ext)
+        for k in range(runs):
+            st, _ = serve.serve(requests, S, tol=1e-8, chunk=16,
+                                check=check_fn if k == runs - 1 else None)
+            stats.append(st)
+        t1.record(ext)
+        torch.cuda.synchronize(dev)
+    c1 = S.counters()
+    out = {"ms": t0.elapsed_time(t1), "stats": stats, "ctr0": c0, "ctr1": c1,
+           "max_true_residual": max(errs) if errs else None, "clocks": clk.summary()}
+    if with_plain:
+        pst, _ = serve.serve_plain(requests, tol=1e-8)
+        out["plain"] = pst
+    return out
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+
+    from num_b200 import serve
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    requests = serve.make_requests(args.requests, rate=args.rate, seed=4)
+    barrier(world)
+    r = serve_measure(dev, requests, args.steps, args.warmup, args.arena_gb * 1e9,
+                      local_rank=local_rank)
+    barrier(world)
+    ms = max_over_ranks([r["ms"]], world, dev)[0]
+    if rank != 0:
+        return None
+    n = len(requests)
+    ms_per = ms / args.steps
+    solves_s = n / (ms_per * 1e-3)
+    c0, c1 = r["ctr0"], r["ctr1"]
+    p50 = statistics.median(s["p50_ms"] for s in r["stats"])
+    p99 = statistics.median(s["p99_ms"] for s in r["stats"])
+    plain = r["plain"]
+    tot_rows = sum(q[1].nrows for q in requests)
+    tot_nnz = sum(q[1].nnz for q in requests)
+    config = {"workload": desc, "name": args.workload, "requests": n,
+              "arrival_rate_per_s": args.rate if args.rate > 0 else "all at t=0 (saturated)",
+              "rows_total": tot_rows, "nnz_total": tot_nnz, "tol": 1e-8,
+              "arena_gb_cap": args.arena_gb, "inner": "fp32 values + vectors, FP64 refinement",
+              "max_true_residual_fp64": r["max_true_residual"],
+              "parallelism": f"replicas x{world}",
+              "api": "num_b200.serve.serve over BatchSolver (nm_solver_* C ABI)"}
+    line = base_line(args, world, round(world * solves_s, 3), "solves/s", ms_per, precision,
+                     config)
+    peak, peak_src = measured_peak()
+    dev_s = (c1["s_device"] - c0["s_device"]) / args.steps
+    line.update({
+        "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3)},
+        "plain_fp64_drop_in": {"solves_per_s": round(plain["solves_per_s"], 3),
+                               "p50_ms": round(plain["p50_ms"], 3),
+                               "p99_ms": round(plain["p99_ms"], 3),
+                               "api": "kokkos_spmv.upload_csr + cg_solve_local, one request at "
+                                      "a time in arrival order"},
+        "ratio_vs_plain": round(solves_s / plain["solves_per_s"], 3),
+        "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s",
+                     "frac": None, "peak_source": peak_src, "traffic": None,
+                     "kernel": "served engine steps",
+                     "device_busy_frac": round(dev_s / (ms_per * 1e-3), 4)},
+        "e2e": {"value": round(world * solves_s, 3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(tot_nnz * 16 + tot_rows * 12),
+                "d2h_bytes_per_step": int(tot_rows * 8),
+                "note": "the served loop is end to end by construction: every request's "
+                        "matrix and b come from host memory and x goes back"},
+        "gpu_launches": int((c1["inner_iterations"] - c0["inner_iterations"]) * 3 +
+                            (c1["outer_launches"] - c0["outer_launches"]) * 6),
+        "clocks": r["clocks"],
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_serve(requests, budget_s=args.cpu_seconds)
+    return line
+
+
+def secondary(local_rank):
+    """Short CG and serving numbers for the default line."""
+    import torch
+
+    from num_b200 import serve
+    dev = torch.device("cuda", local_rank)
+    out = {}
+    r = cg_c1_measure(dev, 20, 3, with_clock=False)
+    out["cg_c1_plain_fp64"] = {"solves_per_s": round(20e3 / r["ms"], 2),
+                               "us_per_iteration": round(r["ms"] * 1e3 / r["iters"], 3),
+                               "iters": r["info"]["iters"], "residual": r["info"]["residual"],
+                               "e2e_solves_per_s": round(1e3 / r["e2e_ms"], 2)}
+    requests = serve.make_requests(200, rate=0.0, seed=4)
+    s = serve_measure(dev, requests, 1, 1, 64e9)
+    st = s["stats"][0]
+    out["serve_c5_sample"] = {
+        "requests": 200, "arrivals": "all at t=0 (saturated)",
+        "served_fp32_ir_solves_per_s": round(200 / (s["ms"] * 1e-3), 2),
+        "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
+        "plain_fp64_solves_per_s": round(s["plain"]["solves_per_s"], 2),
+        "plain_p50_ms": round(s["plain"]["p50_ms"], 2),
+        "plain_p99_ms": round(s["plain"]["p99_ms"], 2),
+        "ratio_vs_plain": round(200 / (s["ms"] * 1e-3) / s["plain"]["solves_per_s"], 3),
+        "max_true_residual_fp64": s["max_true_residual"]}
+    return out
+
+
+# ---- CPU legs (oracle port of the reference's CPU path) --------------------------------------
 
 def cpu_spmv_setup(A, x, precision):
     from oracle import oracle
@@ -323,7 +755,7 @@ def slice_bytes(A, r0, r1, precision):
     return (vb + 4) * nz + 4 * (r1 - r0 + 1) + vb * (r1 - r0) * 2
 
 
-def cpu_baseline(A, x, precision, budget_s=10.0):
+def cpu_baseline_spmv(A, x, precision, budget_s=10.0):
     run, keep, oracle = cpu_spmv_setup(A, x, precision)
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
@@ -342,72 +774,170 @@ def cpu_baseline(A, x, precision, budget_s=10.0):
                       f"{med * 1e3:.2f} ms; oracle/oracle.c or_spmv_*_omp (OpenMP static rows)"}
 
 
-def run_reference(args, rank, world):
-    if rank != 0:
-        return None
-    desc, precision = WORKLOADS[args.workload]
-    A, x = make_workload(args.workload)
-    run, keep, oracle = cpu_spmv_setup(A, x, precision)
+def cpu_baseline_cg(A, b, tol, budget_s=10.0, precond=False, full_iters=None):
+    """Threaded CPU CG (oracle/oracle.c or_cg_omp).  When one solve would take
+    longer than the budget, a capped number of iterations is timed and the
+    solve time scaled to the full iteration count."""
+    from oracle import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     t = time.perf_counter()
-    run(0, A.nrows)
-    full = time.perf_counter() - t
-    per_step = 60.0 / max(1, args.steps + args.warmup)
-    rows = int(max(1024, min(A.nrows, A.nrows * per_step / max(full, 1e-9))))
-    pos = 0
+    info, _ = oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=tol, max_iter=20,
+                            precond=precond)
+    t20 = (time.perf_counter() - t) / max(1, info["iters"])
+    est_iters = full_iters or 1000
+    if t20 * est_iters < budget_s / 3:
+        times, iters = [], None
+        t_end = time.perf_counter() + budget_s
+        while time.perf_counter() < t_end and len(times) < 200:
+            t = time.perf_counter()
+            info, _ = oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=tol, max_iter=20000,
+                                    precond=precond)
+            times.append(time.perf_counter() - t)
+            iters = info["iters"]
+        med = statistics.median(times)
+        sample = (f"{len(times)} full solves ({iters} iterations each) in ~{budget_s:.0f} s, "
+                  f"median {med * 1e3:.2f} ms")
+    else:
+        cap = max(5, int(budget_s / 2 / max(t20, 1e-9)))
+        t = time.perf_counter()
+        info, _ = oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=1e-300, max_iter=cap,
+                                precond=precond)
+        per_it = (time.perf_counter() - t) / cap
+        med = per_it * est_iters
+        sample = (f"{cap} iterations timed ({per_it * 1e3:.2f} ms each), scaled to the "
+                  f"{est_iters} iterations of the full solve")
+    kind = "Jacobi PCG" if precond else "CG"
+    return {"value": round(1.0 / med, 4), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{sample}; oracle/oracle.c or_cg_omp ({kind}, OpenMP loops)"}
 
-    def step():
-        nonlocal pos
-        r0 = pos
-        r1 = min(A.nrows, r0 + rows)
-        run(r0, r1)
-        pos = 0 if r1 >= A.nrows else r1
-        return slice_bytes(A, r0, r1, precision)
 
-    for _ in range(args.warmup):
-        step()
-    tot_b = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        tot_b += step()
+def cpu_baseline_serve(requests, budget_s=10.0):
+    """Threaded CPU Jacobi-PCG of the requests one at a time, in arrival order,
+    for about budget_s seconds."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    order = sorted(range(len(requests)), key=lambda i: requests[i][0])
+    done, t0 = 0, time.perf_counter()
+    for i in order:
+        _, A, b, _ = requests[i]
+        oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=1e-8, max_iter=100000, precond=True)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
     el = time.perf_counter() - t0
-    val = tot_b / el / 1e9
-    sample = (f"row slices of {rows} of {A.nrows} rows per step ({rows / A.nrows:.1%} of one SpMV), "
-              f"oracle/oracle.c or_spmv_*_omp on {threads} threads (the reference's Kokkos-OpenMP "
-              f"build is not buildable here)")
+    return {"value": round(done / el, 3), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"the first {done} of {len(requests)} requests in arrival order, solved "
+                      f"one at a time in {el:.1f} s (oracle/oracle.c or_cg_omp, Jacobi PCG)"}
+
+
+# ---- the reference arm ---------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    desc, kind, precision = WORKLOADS[args.workload]
+    threads = os.cpu_count() or 1
+    note = "the reference's Kokkos-OpenMP build is not buildable here; oracle/oracle.c port"
+    if kind == "spmv":
+        A, x = make_workload(args.workload)
+        if isinstance(A, list):
+            A = block_diagonal(A)
+        run, keep, oracle = cpu_spmv_setup(A, x, precision)
+        oracle.set_threads(threads)
+        t = time.perf_counter()
+        run(0, A.nrows)
+        full = time.perf_counter() - t
+        per_step = 60.0 / max(1, args.steps + args.warmup)
+        rows = int(max(1024, min(A.nrows, A.nrows * per_step / max(full, 1e-9))))
+        pos = 0
+
+        def step():
+            nonlocal pos
+            r0 = pos
+            r1 = min(A.nrows, r0 + rows)
+            run(r0, r1)
+            pos = 0 if r1 >= A.nrows else r1
+            return slice_bytes(A, r0, r1, precision)
+
+        for _ in range(args.warmup):
+            step()
+        tot_b = 0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            tot_b += step()
+        el = time.perf_counter() - t0
+        val, unit = tot_b / el / 1e9, "GB/s"
+        sample = (f"row slices of {rows} of {A.nrows} rows per step ({rows / A.nrows:.1%} of one "
+                  f"SpMV), or_spmv_*_omp on {threads} threads ({note})")
+        cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz}
+        ms_step = el / args.steps * 1e3
+    elif kind in ("cg", "engine"):
+        from num_b200 import generators as gen
+        if kind == "cg":
+            A, _ = make_workload("cg_c1")
+            b, tol, pre, iters = A.to_scipy() @ np.ones(A.ncols), 1e-8, False, None
+        else:
+            A, b = gen.varcoef_poisson_3d(128, seed=3)
+            tol, pre, iters = 1e-10, True, 692
+        per_step_budget = 60.0 / max(1, args.steps + args.warmup)
+        cb = cpu_baseline_cg(A, b, tol, budget_s=per_step_budget * args.steps, precond=pre,
+                             full_iters=iters)
+        val, unit, sample = cb["value"], "solves/s", cb["sample"] + f" ({note})"
+        cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz}
+        ms_step = 1e3 / val
+    else:  # serve
+        from num_b200 import serve
+        requests = serve.make_requests(args.requests, rate=args.rate, seed=4)
+        cb = cpu_baseline_serve(requests, budget_s=60.0)
+        val, unit, sample = cb["value"], "solves/s", cb["sample"] + f" ({note})"
+        cfg = {"workload": desc, "name": args.workload, "requests": len(requests)}
+        ms_step = 1e3 / val
+    cfg["parallelism"] = "cpu"
     return {
-        "metric": METRIC, "value": round(val, 3), "unit": "GB/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(el / args.steps * 1e3, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if precision == "fp64" else "f32", "data": "synthetic",
-        "config": {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
-                   "parallelism": "cpu"},
-        "impl": "reference",
-        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+        "metric": METRIC, "value": round(val, 4), "unit": unit, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": dtype_name(precision if kind == "spmv" else "fp64"), "data": "synthetic",
+        "config": cfg, "impl": "reference",
+        "cpu_baseline": {"value": round(val, 4), "unit": unit, "cores": threads, "kind": "port",
                          "sample": sample},
-        "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": round(val, 4), "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+
+
+DEFAULT_STEPS = {"spmv": 2000, "cg": 50, "engine": 5, "serve": 3}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=0, help="0: the workload's default")
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="spmv_c2a", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the CG / serving summary of the default line")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--tile", type=int, default=0, help="row-block tile (0: library default)")
     ap.add_argument("--stages", type=int, default=0, help="TMA pipeline depth (0: default)")
     ap.add_argument("--short-max", type=int, default=0)
     ap.add_argument("--grid-mult", type=int, default=-1)
+    ap.add_argument("--requests", type=int, default=200, help="serve_c5: requests per pass")
+    ap.add_argument("--rate", type=float, default=0.0,
+                    help="serve_c5: Poisson arrival rate (req/s); 0 = all at t=0")
+    ap.add_argument("--arena-gb", type=float, default=64.0, help="serve_c5: arena cap")
     args = ap.parse_args()
+    kind = WORKLOADS[args.workload][1]
+    if args.steps <= 0:
+        args.steps = DEFAULT_STEPS[kind]
     if args.warmup < 3:
         args.warmup = 3
+    if kind in ("engine", "serve") and args.warmup > 3:
+        args.warmup = 3  # whole solves / passes: three are plenty
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -417,16 +947,19 @@ def main():
         if line:
             print(json.dumps(line), flush=True)
         return
+    import torch
+    torch.cuda.set_device(local_rank)
+    from num_b200 import kokkos_spmv as kspmv
+    kspmv.init(local_rank)
     if world > 1:
         import datetime
 
-        import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        line = run_ours(args, rank, world, local_rank)
+        run = {"spmv": run_spmv, "cg": run_cg, "engine": run_engine, "serve": run_serve}[kind]
+        line = run(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -276,6 +276,17 @@ int nm_solver_status(const nm_solver* S, int32_t slot, int32_t* phase, nm_cg_res
 /* Copy the solution to host memory (x_host may be NULL) and free the slot. */
 int nm_solver_take(nm_solver* S, int32_t slot, double* x_host);
 
+/* Solve an admitted system again (same matrix): b_host (NULL: keep b) and
+ * x0_host (NULL: zero) are copied in, the iteration state is reset, and the
+ * system rejoins at the next step.  Not between step_begin and step_end. */
+int nm_solver_resolve(nm_solver* S, int32_t slot, const double* b_host, const double* x0_host);
+
+/* Copy of a system's current x (the system stays admitted).  Synchronous. */
+int nm_solver_solution(nm_solver* S, int32_t slot, double* x_host);
+
+/* The cudaStream_t the solver's steps run on (for timing with events). */
+int nm_solver_stream(const nm_solver* S, void** stream);
+
 /* Largest free row and nonzero ranges, active systems, free slots. */
 int nm_solver_info(const nm_solver* S, int64_t* free_rows, int64_t* free_nnz, int32_t* active,
                    int32_t* free_slots);

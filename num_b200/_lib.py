@@ -82,6 +82,9 @@ _SIGNATURES = {
     "nm_solver_admit_batch": ([vp, i32, vp, vp, vp, vp, vp, dbl, i32, P_i32, P_i32], C.c_int),
     "nm_solver_step": ([vp, i32, P_i32], C.c_int),
     "nm_solver_step_begin": ([vp, i32], C.c_int),
+    "nm_solver_resolve": ([vp, i32, vp, vp], C.c_int),
+    "nm_solver_stream": ([vp, C.POINTER(vp)], C.c_int),
+    "nm_solver_solution": ([vp, i32, vp], C.c_int),
     "nm_solver_step_end": ([vp, P_i32], C.c_int),
     "nm_solver_counters_get": ([vp, vp], C.c_int),
     "nm_solver_status": ([vp, i32, P_i32, C.POINTER(CgResult), P_i32], C.c_int),

@@ -585,6 +585,7 @@ struct RangeAlloc {
 };
 
 struct HostSys {
+    SysState init{};  // state at admission (nm_solver_resolve starts from it)
     bool used = false;
     int64_t row0 = 0, nrows_alloc = 0, z0 = 0, nnz_alloc = 0;
     int32_t n = 0;
@@ -1258,6 +1259,7 @@ int job_commit(nm_solver* S, AdmitJob& J) {
     h.phase = kSysOuter;
     h.blocks = std::move(J.blocks);
     h.tiles = std::move(J.tiles);
+    h.init = *ss;
     S->lists_dirty = true;
     return NM_OK;
 }
@@ -1554,6 +1556,63 @@ extern "C" int nm_solver_take(nm_solver* S, int32_t slot, double* x_host) {
                                 cudaMemcpyHostToDevice, S->stream));
     NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
     if (was_active) S->lists_dirty = true;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_resolve(nm_solver* S, int32_t slot, const double* b_host,
+                                 const double* x0_host) {
+    using namespace nm;
+    clear_error();
+    if (!S || slot < 0 || slot >= S->cap_sys || !S->sys[slot].used)
+        return fail(NM_ERR_INVALID, "nm_solver_resolve: no system in slot %d", slot);
+    if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_resolve: a step is running");
+    HostSys& h = S->sys[slot];
+    SysState ss = h.init;
+    const size_t n = size_t(h.n);
+    NM_CUDA_TRY(cudaStreamSynchronize(S->up));
+    if (b_host) {
+        double bb = 0.0;
+        for (size_t i = 0; i < n; ++i) bb += b_host[i] * b_host[i];
+        ss.bnorm = bb > 0.0 ? std::sqrt(bb) : 1.0;
+        h.init.bnorm = ss.bnorm;
+        NM_CUDA_TRY(cudaMemcpyAsync(S->b + h.row0, b_host, sizeof(double) * n,
+                                    cudaMemcpyHostToDevice, S->stream));
+    }
+    if (x0_host) {
+        NM_CUDA_TRY(cudaMemcpyAsync(S->x + h.row0, x0_host, sizeof(double) * n,
+                                    cudaMemcpyHostToDevice, S->stream));
+    } else {
+        NM_CUDA_TRY(cudaMemsetAsync(S->x + h.row0, 0, sizeof(double) * n, S->stream));
+    }
+    const size_t tb = inner_bytes(S->inner);
+    NM_CUDA_TRY(cudaMemsetAsync(static_cast<unsigned char*>(S->d) + tb * size_t(h.row0), 0, tb * n,
+                                S->stream));
+    S->h_st[slot] = ss;
+    NM_CUDA_TRY(cudaMemcpyAsync(S->st + slot, &S->h_st[slot], sizeof(SysState),
+                                cudaMemcpyHostToDevice, S->stream));
+    NM_CUDA_TRY(cudaStreamSynchronize(S->stream));  // the host copies may go away
+    if (h.phase != kSysOuter) S->lists_dirty = true;
+    h.phase = kSysOuter;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_solution(nm_solver* S, int32_t slot, double* x_host) {
+    using namespace nm;
+    clear_error();
+    if (!S || !x_host || slot < 0 || slot >= S->cap_sys || !S->sys[slot].used)
+        return fail(NM_ERR_INVALID, "nm_solver_solution: no system in slot %d", slot);
+    if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_solution: a step is running");
+    const HostSys& h = S->sys[slot];
+    NM_CUDA_TRY(cudaMemcpyAsync(x_host, S->x + h.row0, sizeof(double) * size_t(h.n),
+                                cudaMemcpyDeviceToHost, S->stream));
+    NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    return NM_OK;
+}
+
+extern "C" int nm_solver_stream(const nm_solver* S, void** stream) {
+    nm::clear_error();
+    if (!S || !stream) return fail(NM_ERR_INVALID, "nm_solver_stream: NULL argument");
+    *stream = S->stream;
     return NM_OK;
 }
 

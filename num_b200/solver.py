@@ -184,6 +184,35 @@ class BatchSolver:
         self.active.discard(slot)
         return x, info
 
+    def resolve(self, slot: int, b=None, x0=None) -> None:
+        """Solve the admitted system in `slot` again: new b (None keeps it),
+        x0 (None: zero); it rejoins at the next step."""
+        bp = x0p = None
+        if b is not None:
+            b = np.ascontiguousarray(b, np.float64)
+            if b.shape[0] != self.n[slot]:
+                raise ValueError("resolve: b length != n")
+            bp = b.ctypes.data
+        if x0 is not None:
+            x0 = np.ascontiguousarray(x0, np.float64)
+            if x0.shape[0] != self.n[slot]:
+                raise ValueError("resolve: x0 length != n")
+            x0p = x0.ctypes.data
+        _lib.check(self.lib.nm_solver_resolve(self._h, int(slot), bp, x0p), "resolve")
+        self.active.add(slot)
+
+    def solution(self, slot: int) -> np.ndarray:
+        """Copy of a system's current x (the slot stays admitted)."""
+        x = np.empty(self.n[slot], np.float64)
+        _lib.check(self.lib.nm_solver_solution(self._h, int(slot), x.ctypes.data), "solution")
+        return x
+
+    def stream(self) -> int:
+        """cudaStream_t of the solver's steps (an integer handle)."""
+        h = C.c_void_p()
+        _lib.check(self.lib.nm_solver_stream(self._h, C.byref(h)), "stream")
+        return h.value or 0
+
     def counters(self) -> dict:
         """Engine counters (nm_solver_counters_get)."""
         c = _lib.SolverCounters()

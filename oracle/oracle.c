@@ -288,6 +288,79 @@ done:
 }
 
 /* ------------------------------------------------------------------------ */
+/* Threaded CG for the timed CPU baseline only (never a parity reference):   */
+/* the same recurrences as or_cg_local (precond = 0) and or_pcg_jacobi       */
+/* (precond = 1), with every SpMV and vector loop an OpenMP static parallel  */
+/* for, as the reference's Kokkos-OpenMP RangePolicy kernels run on the      */
+/* host (src/spmv_kernel.hpp:170-180, src/vec_ops.hpp:16-69); the dot        */
+/* products reduce in OpenMP's order.                                        */
+/* ------------------------------------------------------------------------ */
+static double omp_dot(int n, const double *x, const double *y)
+{
+    double acc = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : acc)
+    for (int i = 0; i < n; ++i) acc += x[i] * y[i];
+    return acc;
+}
+
+void or_cg_omp(int n, const int32_t *rowptr, const int32_t *colind, const double *vals,
+               const double *b, double *x, double tol, int max_iter, int precond,
+               or_cg_result *res)
+{
+    size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
+    double *r = (double *)malloc(sz), *p = (double *)malloc(sz);
+    double *Ap = (double *)malloc(sz), *z = (double *)malloc(sz);
+    double *dinv = (double *)malloc(sz);
+    if (precond) or_jacobi_dinv(n, rowptr, colind, vals, dinv);
+    or_spmv_f64_omp(n, rowptr, colind, vals, x, Ap);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        r[i] = b[i] - Ap[i];
+        z[i] = precond ? dinv[i] * r[i] : r[i];
+        p[i] = z[i];
+    }
+    double b_norm2 = sqrt(omp_dot(n, b, b));
+    if (b_norm2 == 0.0) b_norm2 = 1.0;
+    double rr = omp_dot(n, r, r);
+    double rz = precond ? omp_dot(n, r, z) : rr;
+    if (sqrt(rr) / b_norm2 < tol) {
+        res->iters = 0; res->final_res = sqrt(rr) / b_norm2; res->converged = 1;
+        goto done;
+    }
+    for (int iter = 0; iter < max_iter; ++iter) {
+        or_spmv_f64_omp(n, rowptr, colind, vals, p, Ap);
+        double alpha = rz / omp_dot(n, p, Ap);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            x[i] = fma(alpha, p[i], x[i]);
+            r[i] = fma(-alpha, Ap[i], r[i]);
+        }
+        rr = omp_dot(n, r, r);
+        double rel = sqrt(rr) / b_norm2;
+        if (rel < tol) {
+            res->iters = iter + 1; res->final_res = rel; res->converged = 1;
+            goto done;
+        }
+        double rz_new = rr;
+        if (precond) {
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+            rz_new = omp_dot(n, r, z);
+        }
+        double beta = rz_new / rz;
+        rz = rz_new;
+        const double *zz = precond ? z : r;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) p[i] = fma(beta, p[i], zz[i]);
+    }
+    res->iters = max_iter;
+    res->final_res = sqrt(omp_dot(n, r, r)) / b_norm2;
+    res->converged = 0;
+done:
+    free(r); free(p); free(Ap); free(z); free(dinv);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Row-block partition ("binning") of the device SpMV.  No counterpart in    */
 /* the reference (its only dispatch input is the global average, see         */
 /* pick_rows_per_team, src/spmv_kernel.hpp:102-109).  This is the CPU        */

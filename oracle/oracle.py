@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
             "or_scale": [C.c_int, C.c_double, vp],
             "or_cg_local": [C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.POINTER(_CgRes)],
             "or_pcg_jacobi": [C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.POINTER(_CgRes)],
+            "or_cg_omp": [C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int,
+                          C.POINTER(_CgRes)],
             "or_jacobi_dinv": [C.c_int, vp, vp, vp, vp],
             "or_row_blocks": [C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp],
             "or_halo_pack": [C.c_int, vp, vp, vp],
@@ -161,6 +163,18 @@ def pcg_jacobi(row_ptr, col_idx, values, b, x0=None, tol=1e-10, max_iter=1000):
     res = _CgRes()
     lib().or_pcg_jacobi(n, _p(rp), _p(ci), _p(v), _p(b), _p(x), float(tol), int(max_iter),
                         C.byref(res))
+    return {"iters": res.iters, "residual": res.final_res, "converged": bool(res.converged)}, x
+
+
+def cg_omp(row_ptr, col_idx, values, b, x0=None, tol=1e-10, max_iter=1000, precond=False):
+    """Threaded CG / Jacobi-PCG (timed CPU baseline, not a parity reference)."""
+    rp, ci, v = _c(row_ptr, np.int32), _c(col_idx, np.int32), _c(values, np.float64)
+    b = _c(b, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    res = _CgRes()
+    lib().or_cg_omp(n, _p(rp), _p(ci), _p(v), _p(b), _p(x), float(tol), int(max_iter),
+                    int(bool(precond)), C.byref(res))
     return {"iters": res.iters, "residual": res.final_res, "converged": bool(res.converged)}, x
 
 

@@ -155,3 +155,26 @@ def test_admit_many_fifo_and_invalid(kspmv):
     for x, info in xs:
         assert info["converged"] and _true_rel(A, x, np.ones(3600)) < 1e-8
     assert np.array_equal(xs[0][0], xs[1][0])
+
+
+def test_resolve_and_solution(kspmv):
+    # A solved system re-solved in place (same b) repeats its bits; with a new
+    # b it converges to the new solution; solution() reads x without freeing.
+    S = _solver("fp32", rows=100_000, nnz=600_000, systems=4)
+    A = gen.laplacian_2d(64)
+    rng = np.random.default_rng(11)
+    b1, b2 = rng.standard_normal(A.nrows), rng.standard_normal(A.nrows)
+    s = S.admit(A, b1, tol=1e-9)
+    while S.active:
+        S.step(8)
+    x1 = S.solution(s)
+    i1 = S.status(s)
+    S.resolve(s)
+    while S.active:
+        S.step(8)
+    assert np.array_equal(S.solution(s), x1) and S.status(s)["iters"] == i1["iters"]
+    S.resolve(s, b=b2)
+    while S.active:
+        S.step(8)
+    x2, i2 = S.take(s)
+    assert i2["converged"] and _true_rel(A, x2, b2) < 1e-9
