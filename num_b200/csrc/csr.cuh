@@ -37,7 +37,10 @@ struct BlockDesc {
     int4 rz;
     int4 xs;
     int4 xl;
-    int4 aux;  // {rows reduced by a warp (nnz > short_max), system slot, 0, 0}
+    // {rows reduced by a warp (nnz > short_max), system slot, 0, 0}; in the
+    // staged copy the SpMV producer sets z = 1 for a block its gate skips and
+    // w = 1 when it staged the x windows
+    int4 aux;
 };
 
 // Kernel-side view of a matrix.

@@ -138,7 +138,7 @@ __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restr
     const bool skip = d.aux.z != 0;
     const bool long_row = z1 - z0 > TILE;
     const bool stage_x = !skip && !long_row && M.stage_x && d.xs.x >= 0;
-    if (!stage_x) d.xs.x = -1;
+    d.aux.w = stage_x ? 1 : 0;  // x windows staged (xs / xl keep the descriptor's values)
     sm.meta[s] = d;
     if (skip || long_row) {  // nothing staged (long rows are read from global)
         mbar_arrive_expect_tx(&sm.full[s], 0u);
@@ -199,50 +199,99 @@ __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int3
 // order; longer rows by a warp.  `ok` = this thread saw the stage complete;
 // a thread that did not touches no staged data but takes the same barriers
 // (the control flow depends only on the descriptor d).
+// Where a gathered block keeps its products: in place of the values when they
+// have the accumulator's width, else (BF16 values, FP32 accumulation) in place
+// of the column indices.
+template <typename V, typename X, typename A, int TILE>
+__device__ __forceinline__ A* prod_slots(SpmvStage<V, X, TILE>& st) {
+    if constexpr (sizeof(V) == sizeof(A)) {
+        return reinterpret_cast<A*>(st.val);
+    } else {
+        static_assert(sizeof(A) == sizeof(int32_t), "products need a 4-byte slot");
+        return reinterpret_cast<A*>(st.col);
+    }
+}
+
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
 __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, const BlockDesc& d,
                                           const X* __restrict__ x,
                                           SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
-    const SpmvStage<V, X, TILE>& st = sm.st[s];
+    SpmvStage<V, X, TILE>& st = sm.st[s];
     const int32_t r0 = d.rz.x, z0 = d.rz.z;
     const int nr = d.rz.y - r0;
     const int32_t a0 = z0 & ~7;
     const int32_t roff = r0 - (r0 & ~3);  // row r0's slot in the staged row_ptr
     // column -> staged x slot: window k holds columns [xs_k, xs_k + xl_k)
-    const bool staged = d.xs.x >= 0;
     const int32_t dl0 = -d.xs.x, dl1 = d.xl.x - d.xs.y, dl2 = d.xl.x + d.xl.y - d.xs.z,
                   dl3 = d.xl.x + d.xl.y + d.xl.z - d.xs.w;
     auto xval = [&](int32_t c) -> A {
-        if (staged) {
-            const int32_t dl = c >= d.xs.w ? dl3 : (c >= d.xs.z ? dl2 : (c >= d.xs.y ? dl1 : dl0));
-            return static_cast<A>(st.xw[c + dl]);
-        }
-        return static_cast<A>(__ldg(x + c));
+        const int32_t dl = c >= d.xs.w ? dl3 : (c >= d.xs.z ? dl2 : (c >= d.xs.y ? dl1 : dl0));
+        return static_cast<A>(st.xw[c + dl]);
     };
+
+    // A block without staged x windows (scattered columns) gathers first:
+    // each consumer reads its share of the block's columns and values into
+    // registers, issues all of its x loads at once, and parks the products
+    // v_j * x[col_j] in the stage; after a consumer barrier the rows add the
+    // products in CSR order (the same operations, in the same order, as
+    // multiplying in the row loop).  Whether a block gathers is decided from
+    // fields the producer leaves unchanged (the descriptor's windows and
+    // M.stage_x), so consumers that gave up on the stage take the same
+    // barrier.
+    const bool gather = !(M.stage_x && d.xs.x >= 0);
+    A* prod = prod_slots<V, X, A, TILE>(st);
+    if (gather) {
+        if (ok) {
+            constexpr int G = (TILE + kConsumers - 1) / kConsumers;
+            const int32_t j0 = z0 - a0 + t, j1 = d.rz.w - a0;
+            int32_t c[G];
+            A v[G], xv[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int32_t j = j0 + g * kConsumers;
+                c[g] = j < j1 ? st.col[j] : 0;
+                v[g] = j < j1 ? widen<V, A>(st.val[j]) : A(0);
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+                if (j0 + g * kConsumers < j1) xv[g] = static_cast<A>(__ldg(x + c[g]));
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int32_t j = j0 + g * kConsumers;
+                if (j < j1) prod[j] = mul_rn(v[g], xv[g]);
+            }
+        }
+        consumer_sync();
+    }
 
     bool is_long = false;
     if (ok && t < nr) {
         const int32_t s0 = st.rp[roff + t] - a0, s1 = st.rp[roff + t + 1] - a0;
         if (s1 - s0 <= M.short_max) {
-            // serial CSR-order sum, operands fetched four at a time
             A acc = A(0);
-            int32_t j = s0;
-            for (; j + 4 <= s1; j += 4) {
-                int32_t c[4];
-                A v[4], xv[4];
+            if (gather) {
+                for (int32_t j = s0; j < s1; ++j) acc = add_rn(acc, prod[j]);
+            } else {
+                // serial CSR-order sum, operands fetched four at a time
+                int32_t j = s0;
+                for (; j + 4 <= s1; j += 4) {
+                    int32_t c[4];
+                    A v[4], xv[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    c[q] = st.col[j + q];
-                    v[q] = widen<V, A>(st.val[j + q]);
+                    for (int q = 0; q < 4; ++q) {
+                        c[q] = st.col[j + q];
+                        v[q] = widen<V, A>(st.val[j + q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) xv[q] = xval(c[q]);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc = add_rn(acc, mul_rn(v[q], xv[q]));
                 }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) xv[q] = xval(c[q]);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc = add_rn(acc, mul_rn(v[q], xv[q]));
+                for (; j < s1; ++j)
+                    acc = add_rn(acc, mul_rn(widen<V, A>(st.val[j]), xval(st.col[j])));
             }
-            for (; j < s1; ++j) acc = add_rn(acc, mul_rn(widen<V, A>(st.val[j]), xval(st.col[j])));
             epi(r0 + t, acc);
         } else {
             is_long = true;
@@ -270,8 +319,12 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
         A acc = A(0);
         if (ok) {
             const int32_t s0 = st.rp[roff + tt] - a0, s1 = st.rp[roff + tt + 1] - a0;
-            for (int32_t j = s0 + lane; j < s1; j += 32)
-                acc += mul_rn(widen<V, A>(st.val[j]), xval(st.col[j]));
+            if (gather) {
+                for (int32_t j = s0 + lane; j < s1; j += 32) acc += prod[j];
+            } else {
+                for (int32_t j = s0 + lane; j < s1; j += 32)
+                    acc += mul_rn(widen<V, A>(st.val[j]), xval(st.col[j]));
+            }
         }
         acc = warp_sum(acc);
         if (lane == 0 && ok) epi(r0 + tt, acc);
