@@ -58,7 +58,7 @@ struct SysState {
     // dynamic
     int32_t phase, it_total, it_inner, outer;
     int32_t converged, pad_;
-    double rnorm, rr0, rr, beta, final_res;
+    double rnorm, rr0, rr, alpha, beta, final_res;
     double rzp[2];      // r.z of the current inner iteration, alternating by iteration parity
     double rnorm_prev;  // scale of the previous inner solve
     double rz_keep;     // r.z of the last completed iteration of the previous inner solve
@@ -69,12 +69,21 @@ struct SysRef {
     int32_t slot, blk0, blk1, tile0, tile1, pad_[3];
 };
 
-// Counts of the device-side work lists.
+// Counts of the device-side work lists (bsys: the large systems of the inner
+// list, whose scalars one CTA per system reduces).
 struct ListHdr {
-    int32_t iblk, itile, isys, oblk, otile, osys, pad_[2];
+    int32_t iblk, itile, isys, oblk, otile, osys, bsys, pad_;
 };
 
 constexpr int kTileRows = 2048;  // rows per vector-kernel tile (within one system)
+
+// A system is "large" when re-reducing its block sums in every tile CTA would
+// cost more than a couple of loads per thread: its alpha and beta are then
+// reduced once, by one CTA (bs_alpha / bs_beta), and the tile kernels read
+// them.  Tiles of a large system carry w = 1.  The choice depends only on the
+// system's own size, so a system takes the same path alone and in any mix.
+constexpr int kLargeBlocks = 512;
+constexpr int kLargeTiles = 256;
 
 __device__ __forceinline__ int32_t sys_phase(const SysState* sys, int32_t slot) {
     return __ldcg(&sys[slot].phase);
@@ -289,6 +298,54 @@ __global__ void __launch_bounds__(kScalarThreads)
     }
 }
 
+// Large systems, inner iteration: alpha = r.z / p.Ap from the block sums
+// (after the SpMV), and the stopping test and beta from the tile sums (after
+// the update), one CTA per system; the same formulas as the tile kernels use
+// for small systems.
+__global__ void __launch_bounds__(kScalarThreads)
+    bs_alpha(const SysRef* list, const int32_t* count, SysState* sys, const double* part_blk,
+             int par) {
+    __shared__ double2 red[kScalarThreads / 32 + 1];
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const SysRef ref = list[i];
+        SysState& S = sys[ref.slot];
+        if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
+        const double pAp = ordered_sum_all<false>(part_blk, ref.blk0, ref.blk1, red).x;
+        if (threadIdx.x == 0) S.alpha = pAp != 0.0 ? __ldcg(&S.rzp[par]) / pAp : 0.0;
+        __syncthreads();  // red is reused by the next system
+    }
+}
+
+__global__ void __launch_bounds__(kScalarThreads)
+    bs_beta(const SysRef* list, const int32_t* count, SysState* sys, const double* part_tile,
+            int par) {
+    __shared__ double2 red[kScalarThreads / 32 + 1];
+    const int32_t n = __ldcg(count);
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const SysRef ref = list[i];
+        SysState& S = sys[ref.slot];
+        if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
+        const double2 t = ordered_sum_all<true>(part_tile, ref.tile0, ref.tile1, red);
+        if (threadIdx.x == 0) {
+            const double inner_rel = sqrt(t.y / S.rr0);
+            const double est = S.rnorm * sqrt(t.y) / S.bnorm;
+            const bool stop = !(inner_rel > S.inner_rtol) || !(est >= S.stop_frac * S.tol) ||
+                              S.it_total >= S.max_iter;
+            const double rz_old = S.rzp[par];
+            S.rr = t.y;
+            if (stop) {
+                S.rz_keep = rz_old;
+                S.phase = kSysOuter;
+            } else {
+                S.beta = t.x / rz_old;
+                S.rzp[par ^ 1] = t.x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ---- per-row vector steps over tiles {row0, row1, slot} ----------------------------
 //
 // A tile is up to kTileRows consecutive rows of one system; tiles start on
@@ -436,10 +493,16 @@ __global__ void __launch_bounds__(kThreads)
                 vload(dinv, row, mv[k]);
             }
         }
-        const int2 br = __ldg(sblk + slot);
-        const double pAp = ordered_sum_all<false>(part_blk, br.x, br.y, red).x;
-        const double rz_old = __ldcg(&sys[slot].rzp[par]);
-        const T alpha = T(pAp != 0.0 ? rz_old / pAp : 0.0);
+        double alpha_d;
+        if (tl.w) {  // large system: bs_alpha reduced it
+            alpha_d = __ldcg(&sys[slot].alpha);
+        } else {
+            const int2 br = __ldg(sblk + slot);
+            const double pAp = ordered_sum_all<false>(part_blk, br.x, br.y, red).x;
+            const double rz_old = __ldcg(&sys[slot].rzp[par]);
+            alpha_d = pAp != 0.0 ? rz_old / pAp : 0.0;
+        }
+        const T alpha = T(alpha_d);
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
             const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
@@ -500,6 +563,20 @@ __global__ void __launch_bounds__(kThreads)
             vload(z, row, zv[k]);
             vload(p, row, pv[k]);
         }
+    }
+    if (tl.w) {  // large system: bs_beta ran the test and set beta (phase above)
+        const T beta = T(__ldcg(&sys[slot].beta));
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
+            if (row < tl.y) {
+                const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
+#pragma unroll
+                for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
+                vstore(p, row, pv[k], valid);
+            }
+        }
+        return;
     }
     const int2 tr = __ldg(stile + slot);
     const double2 t = ordered_sum_all<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
@@ -620,7 +697,7 @@ struct nm_solver {
     nm::ListHdr* h_hdr = nullptr;
     nm::BlockDesc *iblk = nullptr, *oblk = nullptr;
     int4 *itile = nullptr, *otile = nullptr;
-    nm::SysRef *isys = nullptr, *osys = nullptr;
+    nm::SysRef *isys = nullptr, *osys = nullptr, *bsys = nullptr;
     int64_t cap_blk = 0, cap_tile = 0;
     double *part_blk = nullptr, *part_tile = nullptr;
     int2 *sblk = nullptr, *stile = nullptr;                // per slot ranges in the inner lists
@@ -655,7 +732,7 @@ nm_solver::~nm_solver() {
     cudaFree(p); cudaFree(Ap); cudaFree(r); cudaFree(z); cudaFree(d); cudaFree(dinv);
     cudaFree(st); cudaFreeHost(h_st);
     cudaFree(hdr); cudaFreeHost(h_hdr);
-    cudaFree(iblk); cudaFree(oblk); cudaFree(itile); cudaFree(otile); cudaFree(isys); cudaFree(osys);
+    cudaFree(iblk); cudaFree(oblk); cudaFree(itile); cudaFree(otile); cudaFree(isys); cudaFree(osys); cudaFree(bsys);
     cudaFree(part_blk); cudaFree(part_tile);
     cudaFree(sblk); cudaFree(stile);
     cudaFreeHost(h_sblk); cudaFreeHost(h_stile);
@@ -722,7 +799,8 @@ int upload_lists(nm_solver* S) {
     int4* to = S->h_tile + S->cap_tile;
     SysRef* ri = S->h_ref;
     SysRef* ro = S->h_ref + S->cap_sys;
-    int32_t cb_i = 0, ct_i = 0, cs_i = 0, cb_o = 0, ct_o = 0, cs_o = 0;
+    SysRef* rb = S->h_ref + 2 * int64_t(S->cap_sys);
+    int32_t cb_i = 0, ct_i = 0, cs_i = 0, cb_o = 0, ct_o = 0, cs_o = 0, cs_b = 0;
     for (int32_t slot = 0; slot < S->cap_sys; ++slot) {
         HostSys& h = S->sys[slot];
         if (!h.used || (h.phase != kSysInner && h.phase != kSysOuter)) continue;
@@ -735,6 +813,7 @@ int upload_lists(nm_solver* S) {
         cb_i = a.blk1;
         ct_i = a.tile1;
         ri[cs_i++] = a;
+        if (!h.tiles.empty() && h.tiles[0].w) rb[cs_b++] = a;
         if (h.phase == kSysOuter) {
             SysRef o{slot, cb_o, cb_o + int32_t(h.blocks.size()), ct_o,
                      ct_o + int32_t(h.tiles.size()), {0, 0, 0}};
@@ -746,7 +825,7 @@ int upload_lists(nm_solver* S) {
         }
     }
     cudaStream_t s = S->stream;
-    *S->h_hdr = ListHdr{cb_i, ct_i, cs_i, cb_o, ct_o, cs_o, {0, 0}};
+    *S->h_hdr = ListHdr{cb_i, ct_i, cs_i, cb_o, ct_o, cs_o, cs_b, 0};
     NM_CUDA_TRY(cudaMemcpyAsync(S->hdr, S->h_hdr, sizeof(ListHdr), cudaMemcpyHostToDevice, s));
     if (cb_i) NM_CUDA_TRY(cudaMemcpyAsync(S->iblk, bi, sizeof(BlockDesc) * cb_i, cudaMemcpyHostToDevice, s));
     if (cb_o) NM_CUDA_TRY(cudaMemcpyAsync(S->oblk, bo, sizeof(BlockDesc) * cb_o, cudaMemcpyHostToDevice, s));
@@ -754,6 +833,7 @@ int upload_lists(nm_solver* S) {
     if (ct_o) NM_CUDA_TRY(cudaMemcpyAsync(S->otile, to, sizeof(int4) * ct_o, cudaMemcpyHostToDevice, s));
     if (cs_i) NM_CUDA_TRY(cudaMemcpyAsync(S->isys, ri, sizeof(SysRef) * cs_i, cudaMemcpyHostToDevice, s));
     if (cs_o) NM_CUDA_TRY(cudaMemcpyAsync(S->osys, ro, sizeof(SysRef) * cs_o, cudaMemcpyHostToDevice, s));
+    if (cs_b) NM_CUDA_TRY(cudaMemcpyAsync(S->bsys, rb, sizeof(SysRef) * cs_b, cudaMemcpyHostToDevice, s));
     NM_CUDA_TRY(cudaMemcpyAsync(S->sblk, S->h_sblk, sizeof(int2) * size_t(S->cap_sys),
                                 cudaMemcpyHostToDevice, s));
     NM_CUDA_TRY(cudaMemcpyAsync(S->stile, S->h_stile, sizeof(int2) * size_t(S->cap_sys),
@@ -812,6 +892,7 @@ int launch_inner_iters(nm_solver* S, int iters) {
     const ListHdr& h = *S->h_hdr;
     const int g_spmv = fit_grid(S->grid_spmv_inner, h.iblk);
     const int g_vec = fit_grid(INT32_MAX, h.itile);  // one CTA per tile
+    const int g_big = h.bsys > 0 ? fit_grid(S->grid_scalar, h.bsys) : 0;
     const CsrView<V> M = arena_view<V>(S, S->vin ? S->vin : S->v64, S->iblk, &H->iblk);
     constexpr size_t smem = spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>();
     T* p = static_cast<T*>(S->p);
@@ -825,9 +906,13 @@ int launch_inner_iters(nm_solver* S, int iters) {
         const int par = it & 1;
         bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
                                                               S->err);
+        if (g_big) bs_alpha<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                             S->part_blk, par);
         bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->sblk, S->stile,
                                                 S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
                                                 par);
+        if (g_big) bs_beta<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                            S->part_tile, par);
         bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
                                                  S->part_tile, z, p, par);
     }
@@ -870,6 +955,8 @@ int prepare_solver_kernels(nm_solver* S) {
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_update<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pupdate<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pstart<T>));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_alpha));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_beta));
     int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
                             spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
     if (st != NM_OK) return st;
@@ -954,7 +1041,8 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     NM_CUDA_TRY(cudaMallocHost(&S->h_hdr, sizeof(ListHdr)));
     NM_CUDA_TRY(cudaMalloc(&S->isys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->osys, sizeof(SysRef) * size_t(max_systems)));
-    NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 2));
+    NM_CUDA_TRY(cudaMalloc(&S->bsys, sizeof(SysRef) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 3));
     for (int2** r : {&S->sblk, &S->stile}) {
         NM_CUDA_TRY(cudaMalloc(r, sizeof(int2) * size_t(max_systems)));
         NM_CUDA_TRY(cudaMemset(*r, 0, sizeof(int2) * size_t(max_systems)));
@@ -1201,8 +1289,10 @@ void job_prep(const nm_solver* S, AdmitJob& J, bool inner_threads) {
     if (inner_threads) parallel_for(nb, 64, blocks);
     else blocks(0, nb);
     J.tiles.clear();
+    const int32_t ntile = (n + kTileRows - 1) / kTileRows;
+    const int32_t large = (nb > kLargeBlocks || ntile > kLargeTiles) ? 1 : 0;
     for (int32_t t0 = 0; t0 < n; t0 += kTileRows)
-        J.tiles.push_back(make_int4(r0 + t0, r0 + std::min(n, t0 + kTileRows), slot, 0));
+        J.tiles.push_back(make_int4(r0 + t0, r0 + std::min(n, t0 + kTileRows), slot, large));
     std::memset(ss, 0, sizeof(SysState));
     ss->row0 = r0;
     ss->n = n;

@@ -178,3 +178,26 @@ def test_resolve_and_solution(kspmv):
         S.step(8)
     x2, i2 = S.take(s)
     assert i2["converged"] and _true_rel(A, x2, b2) < 1e-9
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_large_system_scalar_path(kspmv, oracle, precision):
+    # A 512^2 Laplacian has more than 512 row blocks, so its alpha / beta are
+    # reduced by one CTA per system instead of in every tile CTA: it must
+    # still converge on the true residual, match the FP64 oracle's iteration
+    # count in FP64 mode, and give the same bits alone and beside small ones.
+    A = gen.laplacian_2d(512)
+    b = np.random.default_rng(12).standard_normal(A.nrows)
+    S = _solver(precision, rows=1_000_000, nnz=6_000_000, systems=16)
+    (x, info), = S.solve([(A, b)], tol=1e-8, max_iter=20000, chunk=16)
+    assert info["converged"] and _true_rel(A, x, b) < 1e-8
+    if precision == "fp64":
+        oinfo, _ = oracle.pcg_jacobi(A.row_ptr, A.col_idx, A.values, b, tol=1e-8,
+                                     max_iter=20000)
+        assert abs(info["iters"] - oinfo["iters"]) <= 2
+    rng = np.random.default_rng(13)
+    mix = [(gen.laplacian_2d(s), None) for s in (20, 33)]
+    mix = [(M, rng.standard_normal(M.nrows)) for M, _ in mix]
+    S2 = _solver(precision, rows=1_000_000, nnz=6_000_000, systems=16)
+    out = S2.solve([mix[0], (A, b), mix[1]], tol=1e-8, max_iter=20000, chunk=16)
+    assert out[1][1]["iters"] == info["iters"] and np.array_equal(out[1][0], x)
