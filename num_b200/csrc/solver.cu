@@ -466,7 +466,7 @@ __host__ __device__ constexpr int kVecIters(int vn) { return kTileRows / (vn * k
 // The system's first tile counts the iteration.  No atomics: step 3 reduces
 // the tile sums.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     bs_update(const int4* tiles, const int32_t* count, SysState* sys, const int2* sblk,
               const int2* stile, const double* part_blk, const T* __restrict__ p,
               const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
@@ -480,48 +480,52 @@ __global__ void __launch_bounds__(kThreads)
     const int32_t slot = tl.z;
     T rz = T(0), rr = T(0);
     if (sys_phase(sys, slot) == kSysInner) {  // phase is not written by this kernel
-        // operands first, so their latency overlaps the block-sum reduction
-        T pv[IT][VN], av[IT][VN], rv[IT][VN], dv[IT][VN], mv[IT][VN];
-#pragma unroll
-        for (int k = 0; k < IT; ++k) {
-            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
-            if (row < tl.y) {
-                vload(p, row, pv[k]);
-                vload(Ap, row, av[k]);
-                vload(r, row, rv[k]);
-                vload(d, row, dv[k]);
-                vload(dinv, row, mv[k]);
-            }
-        }
         double alpha_d;
         if (tl.w) {  // large system: bs_alpha reduced it
             alpha_d = __ldcg(&sys[slot].alpha);
-        } else {
+        } else {  // small system: at most a few block sums per thread
             const int2 br = __ldg(sblk + slot);
             const double pAp = ordered_sum_all<false>(part_blk, br.x, br.y, red).x;
             const double rz_old = __ldcg(&sys[slot].rzp[par]);
             alpha_d = pAp != 0.0 ? rz_old / pAp : 0.0;
         }
         const T alpha = T(alpha_d);
+        // two vectors of each operand per thread in flight at a time
+        constexpr int KB = IT < 2 ? IT : 2;
 #pragma unroll
-        for (int k = 0; k < IT; ++k) {
-            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
-            if (row < tl.y) {
-                const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
-                T zo[VN];
+        for (int k0 = 0; k0 < IT; k0 += KB) {
+            T pv[KB][VN], av[KB][VN], rv[KB][VN], dv[KB][VN], mv[KB][VN];
 #pragma unroll
-                for (int e = 0; e < VN; ++e) {
-                    dv[k][e] = fma(alpha, pv[k][e], dv[k][e]);
-                    rv[k][e] = fma(-alpha, av[k][e], rv[k][e]);
-                    zo[e] = mv[k][e] * rv[k][e];
-                    if (e < valid) {
-                        rz = fma(rv[k][e], zo[e], rz);
-                        rr = fma(rv[k][e], rv[k][e], rr);
-                    }
+            for (int k = 0; k < KB; ++k) {
+                const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
+                if (row < tl.y) {
+                    vload(p, row, pv[k]);
+                    vload(Ap, row, av[k]);
+                    vload(r, row, rv[k]);
+                    vload(d, row, dv[k]);
+                    vload(dinv, row, mv[k]);
                 }
-                vstore(d, row, dv[k], valid);
-                vstore(r, row, rv[k], valid);
-                vstore(z, row, zo, valid);
+            }
+#pragma unroll
+            for (int k = 0; k < KB; ++k) {
+                const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
+                if (row < tl.y) {
+                    const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
+                    T zo[VN];
+#pragma unroll
+                    for (int e = 0; e < VN; ++e) {
+                        dv[k][e] = fma(alpha, pv[k][e], dv[k][e]);
+                        rv[k][e] = fma(-alpha, av[k][e], rv[k][e]);
+                        zo[e] = mv[k][e] * rv[k][e];
+                        if (e < valid) {
+                            rz = fma(rv[k][e], zo[e], rz);
+                            rr = fma(rv[k][e], rv[k][e], rr);
+                        }
+                    }
+                    vstore(d, row, dv[k], valid);
+                    vstore(r, row, rv[k], valid);
+                    vstore(z, row, zo, valid);
+                }
             }
         }
         if (threadIdx.x == 0 && i == __ldg(stile + slot).x) {
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(kThreads)
 // the one write others may see early, and they then skip exactly as the test
 // would make them.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     bs_pupdate(const int4* tiles, const int32_t* count, SysState* sys, const int2* stile,
                const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par) {
     constexpr int VN = Vec16<T>::N;
@@ -555,6 +559,37 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x == 0) phase = sys_phase(sys, slot);
     __syncthreads();
     if (phase != kSysInner) return;  // uniform over the CTA
+    double beta_d;
+    if (tl.w) {  // large system: bs_beta ran the test and set beta (phase above)
+        beta_d = __ldcg(&sys[slot].beta);
+    } else {  // small system: reduce the tile sums and decide, as every CTA of it does
+        const int2 tr = __ldg(stile + slot);
+        const double2 t = ordered_sum_all<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
+        const SysState& S = sys[slot];
+        const double rr0 = __ldcg(&S.rr0), rnorm = __ldcg(&S.rnorm), bnorm = __ldcg(&S.bnorm);
+        const double inner_rel = sqrt(t.y / rr0);
+        const double est = rnorm * sqrt(t.y) / bnorm;  // estimated |b - Ax| / |b|
+        const bool stop = !(inner_rel > __ldcg(&S.inner_rtol)) ||
+                          !(est >= __ldcg(&S.stop_frac) * __ldcg(&S.tol)) ||
+                          __ldcg(&S.it_total) >= __ldcg(&S.max_iter);
+        const bool first = i == tr.x;
+        const double rz_old = __ldcg(&S.rzp[par]);
+        if (stop) {  // stop the inner solve; refine next step
+            if (first && threadIdx.x == 0) {
+                sys[slot].rr = t.y;
+                sys[slot].rz_keep = rz_old;
+                sys[slot].phase = kSysOuter;
+            }
+            return;
+        }
+        beta_d = t.x / rz_old;
+        if (first && threadIdx.x == 0) {
+            sys[slot].rr = t.y;
+            sys[slot].beta = beta_d;
+            sys[slot].rzp[par ^ 1] = t.x;
+        }
+    }
+    const T beta = T(beta_d);
     T zv[IT][VN], pv[IT][VN];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
@@ -564,41 +599,6 @@ __global__ void __launch_bounds__(kThreads)
             vload(p, row, pv[k]);
         }
     }
-    if (tl.w) {  // large system: bs_beta ran the test and set beta (phase above)
-        const T beta = T(__ldcg(&sys[slot].beta));
-#pragma unroll
-        for (int k = 0; k < IT; ++k) {
-            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
-            if (row < tl.y) {
-                const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
-#pragma unroll
-                for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
-                vstore(p, row, pv[k], valid);
-            }
-        }
-        return;
-    }
-    const int2 tr = __ldg(stile + slot);
-    const double2 t = ordered_sum_all<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
-    const SysState& S = sys[slot];
-    const double rr0 = __ldcg(&S.rr0), rnorm = __ldcg(&S.rnorm), bnorm = __ldcg(&S.bnorm);
-    const double inner_rel = sqrt(t.y / rr0);
-    const double est = rnorm * sqrt(t.y) / bnorm;  // estimated |b - Ax| / |b|
-    const bool stop = !(inner_rel > __ldcg(&S.inner_rtol)) ||
-                      !(est >= __ldcg(&S.stop_frac) * __ldcg(&S.tol)) ||
-                      __ldcg(&S.it_total) >= __ldcg(&S.max_iter);
-    const bool first = i == tr.x;
-    const double rz_old = __ldcg(&S.rzp[par]);
-    if (stop) {  // stop the inner solve; refine next step
-        if (first && threadIdx.x == 0) {
-            sys[slot].rr = t.y;
-            sys[slot].rz_keep = rz_old;
-            sys[slot].phase = kSysOuter;
-        }
-        return;
-    }
-    const double beta_d = t.x / rz_old;
-    const T beta = T(beta_d);
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
         const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
@@ -608,11 +608,6 @@ __global__ void __launch_bounds__(kThreads)
             for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
             vstore(p, row, pv[k], valid);
         }
-    }
-    if (first && threadIdx.x == 0) {
-        sys[slot].rr = t.y;
-        sys[slot].beta = beta_d;
-        sys[slot].rzp[par ^ 1] = t.x;
     }
 }
 
