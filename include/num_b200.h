@@ -175,6 +175,13 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
 
 /* ---- CG -------------------------------------------------------------------- */
 
+/* Process-wide choice of how nm_cg_local / nm_dist_cg_single iterate:
+ * 1 (default) one persistent cooperative launch per solve when the device
+ * supports it and the matrix's SpMV grid is co-resident; 0 CUDA-graph chunks
+ * of three kernels per iteration.  Both give the same iterates, bit for bit.
+ * No reference counterpart (an implementation switch). */
+int nm_cg_set_persistent(int32_t enable);
+
 /* cg_solve_local (src/cg_solver.hpp:133-196; src/bindings.cpp:273-290):
  * unpreconditioned CG, x in/out, same stopping rule and iteration count.
  * The iteration runs on the device with device-resident scalars; the

@@ -16,6 +16,7 @@
 // HBM per iteration: 12 nnz + 4(n+1) (matrix) + 8n (p gather, L2-resident
 // in steady state) + 8n (Ap write) in K1; 4 reads + 2 writes of n doubles in
 // K2; 2 reads + 1 write in K3 -- 12 nnz + 4(n+1) + 88 n bytes.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -153,6 +154,208 @@ __global__ void __launch_bounds__(kThreads)
         p[i] = fma(beta, p[i], r[i]);  // p = 1*r + beta*p
 }
 
+// ---------------------------------------------------------------------------
+// Persistent CG: the whole iteration loop in one cooperative launch.
+//
+// The grid is the SpMV grid of the three-kernel path (every CTA resident, so a
+// grid-wide barrier can be met), and each phase reproduces that path exactly:
+//   A  the same SpMV pipeline with the same p.Ap epilogue and CTA sum; every
+//      CTA then reduces the CTA sums in the order the three-kernel path's
+//      last CTA uses (stride blockDim over gridDim);
+//   B  x, r update and r.r over "virtual CTAs" v = blockIdx.x, + gridDim.x,
+//      ... < grid_vec of 256 threads, with cg_update_xr_kernel's element
+//      mapping and CTA sum, and the same final reduction;
+//   C  p = r + beta p (elementwise).
+// So the iterates are bit-identical to nm_cg_local's graph path.  Every CTA
+// computes the scalars itself (identically); CTA 0 publishes the final state.
+// Data written inside the kernel is read with ld.global.cg (L2), never through
+// the non-coherent read-only path.  Three grid barriers per iteration replace
+// the kernel boundaries; each wait is bounded (kWaitLimitNs): a CTA that gives
+// up sets the error word and the state to kCgDeviceError and leaves, and the
+// others give up at their next barrier.
+// ---------------------------------------------------------------------------
+
+// Grid barrier on (count, gen); returns false when the wait gave up or a CTA
+// has marked the solve failed (*status == kCgDeviceError) -- read once, by
+// thread 0, so every thread of the CTA gets the same answer.
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen,
+                                             unsigned int* err, const int32_t* status,
+                                             bool* flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool ok = true;
+        // Arrival is an acq_rel add on count (a release sequence: the last
+        // arriver acquires every CTA's writes); it resets count and releases
+        // gen, on which the others spin with acquire loads.
+        unsigned int g0, prev;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(g0) : "l"(gen) : "memory");
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                     : "=r"(prev) : "l"(count) : "memory");
+        if (prev == gridDim.x - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(count) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(gen) : "memory");
+        } else {
+            const uint64_t t0 = global_timer_ns();
+            for (uint32_t it = 0;; ++it) {
+                unsigned int g;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(gen) : "memory");
+                if (g != g0) break;
+                if ((it & 255u) == 0 && (global_timer_ns() - t0 > kWaitLimitNs || it > (1u << 30))) {
+                    atomicOr(err, kErrWaitTimeout);
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        *flag = ok && __ldcg(status) != kCgDeviceError;
+    }
+    __syncthreads();
+    return *flag;
+}
+
+// Sum over the first 8 warps (the 256 threads of a cg_update_xr_kernel CTA);
+// valid in thread 0.  All threads of the CTA call it.
+__device__ __forceinline__ double block_sum8(double v, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0 && warp < kWarps) scratch[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += scratch[w];
+    }
+    __syncthreads();
+    return s;
+}
+
+struct CoopPApEpi {
+    static constexpr bool kBlockSums = false;
+    double* __restrict__ Ap;
+    const double* __restrict__ p;
+    double dot;
+    __device__ __forceinline__ void operator()(int32_t row, double v) {
+        Ap[row] = v;
+        dot = fma(__ldcg(p + row), v, dot);
+    }
+    __device__ __forceinline__ double take() { return 0.0; }
+    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+};
+
+template <int TILE, int STAGES>
+__global__ void __launch_bounds__(kCtaThreads)
+    cg_coop_kernel(CsrView<double> M, CgState* st, double* p, double* Ap, double* r,
+                   double* part_a, double* part_b, int grid_vec, int64_t n, unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES>*>(smem_raw);
+    __shared__ double bcast[2];
+    __shared__ bool flag;
+    const int t = threadIdx.x;
+    // the state after cg_init_kernel
+    if (__ldcg(&st->done)) return;
+    double* __restrict__ x = st->x;
+    const double bnorm = __ldcg(&st->bnorm), tol = __ldcg(&st->tol);
+    const int32_t max_iter = __ldcg(&st->max_iter), guard = __ldcg(&st->guard);
+    double rr = __ldcg(&st->rr);
+    int32_t iter = __ldcg(&st->iter);
+    M.coherent_x = 1;
+    bool failed = false;
+    for (;;) {
+        // ---- A: Ap = A p, p.Ap ----
+        CoopPApEpi epi{Ap, p, 0.0};
+        const bool ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
+        __syncthreads();
+        if (t == 0) {  // the ring's barriers are initialised again by the next SpMV
+#pragma unroll
+            for (int q = 0; q < STAGES; ++q) {
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&sm.full[q]))
+                             : "memory");
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&sm.empty[q]))
+                             : "memory");
+            }
+        }
+        if (!ok) atomicExch(&st->status, kCgDeviceError);
+        const double pa = block_sum(epi.dot, sm.red);
+        if (t == 0) part_a[blockIdx.x] = pa;
+        if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
+        double s = 0.0;
+        for (unsigned i = t; i < gridDim.x; i += blockDim.x) s += __ldcg(part_a + i);
+        const double pAp = block_sum(s, sm.red);
+        if (t == 0) bcast[0] = pAp;
+        __syncthreads();
+        const double pAp_all = bcast[0];
+        if (guard && fabs(pAp_all) < 1e-300) {
+            if (blockIdx.x == 0 && t == 0) {
+                st->pAp = pAp_all;
+                st->status = kCgBreakdown;
+                st->converged = 0;
+                st->iters = iter;
+                st->final_res = sqrt(rr) / bnorm;
+                st->done = 1;
+            }
+            return;
+        }
+        const double alpha = rr / pAp_all;
+        // ---- B: x += alpha p, r -= alpha Ap, r.r (virtual CTAs of 256 threads) ----
+        for (int v = blockIdx.x; v < grid_vec; v += gridDim.x) {
+            double sv = 0.0;
+            if (t < kThreads) {
+                for (int64_t i = int64_t(v) * kThreads + t; i < n; i += int64_t(grid_vec) * kThreads) {
+                    const double pi = __ldcg(p + i);
+                    x[i] = fma(alpha, pi, __ldcg(x + i));
+                    const double ri = fma(-alpha, __ldcg(Ap + i), __ldcg(r + i));
+                    r[i] = ri;
+                    sv = fma(ri, ri, sv);
+                }
+            }
+            const double pv = block_sum8(sv, sm.red);
+            if (t == 0) part_b[v] = pv;
+        }
+        if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
+        double s2 = 0.0;
+        if (t < kThreads)
+            for (int i = t; i < grid_vec; i += kThreads) s2 += __ldcg(part_b + i);
+        const double rr_new0 = block_sum8(s2, sm.red);
+        if (t == 0) bcast[1] = rr_new0;
+        __syncthreads();
+        const double rr_new = bcast[1];
+        ++iter;
+        const double rel = sqrt(rr_new) / bnorm;
+        if (rel < tol) {
+            if (blockIdx.x == 0 && t == 0) {
+                st->iter = iter; st->converged = 1; st->iters = iter; st->final_res = rel;
+                st->rr = rr_new; st->done = 1;
+            }
+            return;
+        }
+        const double beta = rr_new / rr;
+        rr = rr_new;
+        if (iter >= max_iter) {
+            if (blockIdx.x == 0 && t == 0) {
+                st->iter = iter; st->converged = 0; st->iters = max_iter; st->final_res = rel;
+                st->beta = beta; st->rr = rr; st->done = 1;
+            }
+            return;
+        }
+        // ---- C: p = r + beta p ----
+        for (int64_t i = int64_t(blockIdx.x) * blockDim.x + t; i < n;
+             i += int64_t(gridDim.x) * blockDim.x)
+            p[i] = fma(beta, __ldcg(p + i), __ldcg(r + i));
+        if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
+    }
+    if (failed && t == 0) {
+        atomicExch(&st->status, kCgDeviceError);
+        atomicExch(&st->done, 1);
+    }
+}
+
+namespace {
+std::atomic<int> g_cg_persistent{1};  // nm_cg_set_persistent
+// Largest system solved by the persistent launch; larger ones keep the graph
+// path (their vector phases need more CTAs than the SpMV grid has).
+constexpr int64_t kCoopMaxRows = 262144;
+}  // namespace
+
 CgWorkspace::~CgWorkspace() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -172,6 +375,19 @@ int prepare_cg_spmv(int* occ) {
     return prepare_kernel(reinterpret_cast<const void*>(cg_spmv_pap_kernel<TILE, STAGES>),
                           kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(),
                           occ);
+}
+
+template <int TILE, int STAGES>
+int prepare_coop(int* occ) {
+    return prepare_kernel(reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES>),
+                          kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(),
+                          occ);
+}
+
+template <int TILE>
+int prepare_coop_s(int stages, int* occ) {
+    if (stages == 4) return prepare_coop<TILE, 4>(occ);
+    return stages == 3 ? prepare_coop<TILE, 3>(occ) : prepare_coop<TILE, 2>(occ);
 }
 
 template <int TILE>
@@ -211,6 +427,22 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     if (st != NM_OK) return st;
     ws->grid_spmv = spmv_grid(A, occ);
     ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
+    {
+        // The persistent solve runs on the same grid, every CTA resident.
+        int dev = 0, coop_ok = 0, occ_c = 0;
+        NM_CUDA_TRY(cudaGetDevice(&dev));
+        NM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
+        switch (A->tune.tile) {
+            case 1024: st = prepare_coop_s<1024>(A->tune.stages, &occ_c); break;
+            case 4096: st = prepare_coop_s<4096>(A->tune.stages, &occ_c); break;
+            default: st = prepare_coop_s<2048>(A->tune.stages, &occ_c); break;
+        }
+        if (st != NM_OK) return st;
+        // Large systems keep the graph path: their update phases need more CTAs
+        // than the SpMV grid has.
+        ws->coop = coop_ok && int64_t(occ_c) * sm_count() >= ws->grid_spmv &&
+                   n <= kCoopMaxRows;
+    }
     NM_CUDA_TRY(cudaMalloc(&ws->partials, sizeof(double) * size_t(ws->partials_cap)));
     ws->err = device_error_word();
     if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
@@ -269,6 +501,37 @@ int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* ou
     return NM_OK;
 }
 
+template <int TILE, int STAGES>
+int launch_coop_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    CsrView<double> M = A->view<double>();
+    M.stage_x = 1;  // p is a workspace vector (256-byte aligned)
+    double* part_a = ws->partials;
+    double* part_b = ws->partials + ws->grid_spmv;
+    int grid_vec = ws->grid_vec;
+    int64_t n = ws->n;
+    void* args[] = {&M, &ws->st, &ws->p, &ws->Ap, &ws->r, &part_a, &part_b, &grid_vec, &n,
+                    &ws->err};
+    NM_CUDA_TRY(cudaLaunchCooperativeKernel(
+        reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES>), dim3(ws->grid_spmv),
+        dim3(kCtaThreads), args, spmv_smem_bytes<double, double, double, TILE, STAGES>(), s));
+    return NM_OK;
+}
+
+template <int TILE>
+int launch_coop_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    if (A->tune.stages == 4) return launch_coop_t<TILE, 4>(A, ws, s);
+    if (A->tune.stages == 3) return launch_coop_t<TILE, 3>(A, ws, s);
+    return launch_coop_t<TILE, 2>(A, ws, s);
+}
+
+int launch_coop(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    switch (A->tune.tile) {
+        case 1024: return launch_coop_s<1024>(A, ws, s);
+        case 4096: return launch_coop_s<4096>(A, ws, s);
+        default: return launch_coop_s<2048>(A, ws, s);
+    }
+}
+
 }  // namespace
 
 // Runs one CG solve on `s`; synchronises `s` before returning.
@@ -297,9 +560,17 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
                                                      ws->partials);
     NM_CHECK_LAUNCH();
 
-    // Iterate in graph chunks of growing length; poll `done` in between.
+    const bool coop = ws->coop && g_cg_persistent.load();
+    if (coop) {
+        // the whole iteration loop in one persistent launch
+        st = launch_coop(A, ws, s);
+        if (st != NM_OK) return st;
+        NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+        NM_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    // Otherwise iterate in graph chunks of growing length; poll `done` in between.
     int chunk = 8;
-    for (;;) {
+    for (; !coop;) {
         NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         NM_CUDA_TRY(cudaStreamSynchronize(s));
         if (ws->h_out->done) break;
@@ -323,6 +594,12 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
 }
 
 }  // namespace nm
+
+extern "C" int nm_cg_set_persistent(int32_t enable) {
+    nm::clear_error();
+    nm::g_cg_persistent.store(enable ? 1 : 0);
+    return NM_OK;
+}
 
 extern "C" int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter,
                            nm_cg_result* result, void* stream) {

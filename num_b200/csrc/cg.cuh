@@ -22,6 +22,7 @@ struct CgState {
     double bnorm, rr, pAp, alpha, beta, final_res;
     int32_t iter, done, converged, iters, status;
     unsigned int counter;  // arrival counter of the last-CTA reductions
+    unsigned int bar_count, bar_gen;  // grid barrier of the persistent solve
 };
 
 // Status codes written to CgState::status.
@@ -31,6 +32,7 @@ constexpr int kCgDeviceError = 2;
 
 struct CgWorkspace {
     int64_t n = 0;
+    bool coop = false;  // the persistent cooperative solve fits this matrix's SpMV grid
     double* r = nullptr;
     double* p = nullptr;
     double* Ap = nullptr;

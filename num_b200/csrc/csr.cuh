@@ -55,6 +55,10 @@ struct CsrView {
     int32_t short_max;
     int32_t stage_x;  // 1: x windows are staged (x 16-byte aligned); 0: gather from global
     const int32_t* nblk_dev;  // when set, the block count is read from device memory
+    // 1: x is written by other CTAs of the same kernel (a persistent solver),
+    // so x values not staged by TMA are read through L2 (ld.global.cg), not
+    // the non-coherent read-only path
+    int32_t coherent_x = 0;
 };
 
 // Default row-block parameters.

@@ -172,6 +172,13 @@ __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restr
     }
 }
 
+// x entries that TMA did not stage: the read-only path, or L2 when x changes
+// within the kernel (M.coherent_x).
+template <typename V, typename X>
+__device__ __forceinline__ X load_x(const CsrView<V>& M, const X* p) {
+    return M.coherent_x ? __ldcg(p) : __ldg(p);
+}
+
 // One long row (nnz > TILE) straight from global memory, all consumers.
 template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
 __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int32_t r0,
@@ -187,7 +194,7 @@ __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int3
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int32_t jj = j + q;
-            if (jj >= z0 && jj < z1) s += v[q] * static_cast<A>(__ldg(x + cc[q]));
+            if (jj >= z0 && jj < z1) s += v[q] * static_cast<A>(load_x(M, x + cc[q]));
         }
     }
     s = consumer_sum(s, sm.red);
@@ -256,7 +263,7 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
             }
 #pragma unroll
             for (int g = 0; g < G; ++g)
-                if (j0 + g * kConsumers < j1) xv[g] = static_cast<A>(__ldg(x + c[g]));
+                if (j0 + g * kConsumers < j1) xv[g] = static_cast<A>(load_x(M, x + c[g]));
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int32_t j = j0 + g * kConsumers;

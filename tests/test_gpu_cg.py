@@ -232,3 +232,33 @@ def test_vector_ops_bit_exact(nmlib, kspmv, oracle):
     assert np.array_equal(zt.cpu().numpy(), y)
     zero = C.c_double(7.0)
     assert nmlib.nm_dot(0, None, None, C.byref(zero), s) == 0 and zero.value == 0.0
+
+
+@pytest.mark.parametrize("case", ["lap2d_256", "lap3d_64", "varcoef_48", "banded"])
+def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
+    # nm_cg_local runs the whole solve in one cooperative launch by default;
+    # the three-kernel CUDA-graph path must give the same bits.
+    rng = np.random.default_rng(21)
+    if case == "lap2d_256":
+        A = gen.laplacian_2d(256)
+    elif case == "lap3d_64":
+        A = gen.laplacian_3d(64)
+    elif case == "varcoef_48":
+        A, _ = gen.varcoef_poisson_3d(48, seed=3)
+    else:
+        A = gen.banded_spd(300_000, 5, rng)
+    b = torch.tensor(rng.standard_normal(A.nrows), device="cuda")
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    out = []
+    try:
+        for persistent in (1, 0, 1):
+            nmlib.nm_cg_set_persistent(persistent)
+            x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
+            info = kspmv.cg_solve_local(M, b, x, tol=1e-9, max_iter=3000)
+            out.append((info, x.cpu().numpy()))
+    finally:
+        nmlib.nm_cg_set_persistent(1)
+    for info, x in out[1:]:
+        assert info == out[0][0]
+        assert np.array_equal(x, out[0][1])
+    assert out[0][0]["converged"]
