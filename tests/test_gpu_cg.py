@@ -262,3 +262,20 @@ def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
         assert info == out[0][0]
         assert np.array_equal(x, out[0][1])
     assert out[0][0]["converged"]
+
+
+@pytest.mark.parametrize("offset", [0, 1])
+def test_large_system_graph_path(kspmv, oracle, offset):
+    # 600^2 Laplacian (360,000 rows, above the persistent solve's limit, so
+    # the CUDA-graph path), x 16-byte aligned or one element off: the same
+    # iteration count as the oracle (+-1) and solutions within 1e-9 of it.
+    A = gen.laplacian_2d(600)
+    b = np.random.default_rng(31).standard_normal(A.nrows)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    buf = torch.zeros(A.nrows + 1, dtype=torch.float64, device="cuda")
+    x = buf[offset:offset + A.nrows]
+    info = kspmv.cg_solve_local(M, torch.tensor(b, device="cuda"), x, tol=1e-8, max_iter=5000)
+    oinfo, ox = oracle.cg_local(A.row_ptr, A.col_idx, A.values, b, tol=1e-8, max_iter=5000)
+    assert info["converged"] and abs(info["iters"] - oinfo["iters"]) <= 1
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(xs - ox) <= 1e-9 * np.linalg.norm(ox)
