@@ -246,8 +246,10 @@ int nm_solver_admit_batch(nm_solver* S, int32_t count, const int32_t* const* row
                           const int32_t* n, const double* const* b, double tol, int32_t max_iter,
                           int32_t* slots, int32_t* admitted);
 
-/* One step of the batch: the pending refinement steps, then `iters` inner
- * iterations of every active system (rounded up to an even count), then the
+/* One step of the batch: the pending refinement steps, then up to `iters`
+ * inner iterations of every active system (rounded up to a multiple of 8; in
+ * groups of 8, the device ends the step early once no system is iterating --
+ * every live one has converged or awaits its refinement step), then the
  * systems' states are read back; *n_done = systems that finished in this
  * step.  Synchronous. */
 int nm_solver_step(nm_solver* S, int32_t iters, int32_t* n_done);
@@ -262,7 +264,7 @@ int nm_solver_step_end(nm_solver* S, int32_t* n_done);
 
 /* Engine counters since creation: steps run, list rebuilds, chunk graph
  * captures and full instantiations, outer (refinement) launches, inner
- * iterations enqueued; host seconds spent per part of a step (list upload,
+ * iterations run; host seconds spent per part of a step (list upload,
  * outer launch, capture, waiting in nm_solver_step_end, state scan) and of
  * admission (parallel preparation, upload enqueue); device seconds of all
  * steps and milliseconds of the last one. */
@@ -271,6 +273,7 @@ typedef struct {
         inner_iterations;
     double s_lists, s_outer, s_capture, s_run, s_scan;
     double s_admit_prep, s_admit_commit, s_device, last_step_ms;
+    int64_t last_step_iters;  /* inner iterations the last step ran */
 } nm_solver_counters;
 int nm_solver_counters_get(const nm_solver* S, nm_solver_counters* out);
 

@@ -42,7 +42,8 @@ class SolverCounters(C.Structure):
                                          "inner_iterations")] + \
                [(n, C.c_double) for n in ("s_lists", "s_outer", "s_capture", "s_run", "s_scan",
                                           "s_admit_prep", "s_admit_commit", "s_device",
-                                          "last_step_ms")]
+                                          "last_step_ms")] + \
+               [("last_step_iters", C.c_int64)]
 
 
 class TuneTrial(C.Structure):

@@ -75,6 +75,15 @@ struct ListHdr {
     int32_t iblk, itile, isys, oblk, otile, osys, bsys, pad_;
 };
 
+// Control words of a step's device-side loop: the iterations done so far in
+// this step, systems still iterating after the loop body's last iteration,
+// and the step's iteration cap.  The body is kLoopUnroll iterations (an even
+// number, so the r.z parity of each iteration is fixed in the body).
+struct StepCtl {
+    unsigned int iter, live, cap, pad_;
+};
+
+
 constexpr int kTileRows = 2048;  // rows per vector-kernel tile (within one system)
 
 // A system is "large" when re-reducing its block sums in every tile CTA would
@@ -319,7 +328,7 @@ __global__ void __launch_bounds__(kScalarThreads)
 
 __global__ void __launch_bounds__(kScalarThreads)
     bs_beta(const SysRef* list, const int32_t* count, SysState* sys, const double* part_tile,
-            int par) {
+            int par, StepCtl* ctl) {
     __shared__ double2 red[kScalarThreads / 32 + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
@@ -340,6 +349,7 @@ __global__ void __launch_bounds__(kScalarThreads)
             } else {
                 S.beta = t.x / rz_old;
                 S.rzp[par ^ 1] = t.x;
+                if (ctl) atomicAdd(&ctl->live, 1u);
             }
         }
         __syncthreads();
@@ -547,7 +557,8 @@ __global__ void __launch_bounds__(kThreads, 4)
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
     bs_pupdate(const int4* tiles, const int32_t* count, SysState* sys, const int2* stile,
-               const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par) {
+               const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par,
+               StepCtl* ctl) {
     constexpr int VN = Vec16<T>::N;
     constexpr int IT = kVecIters(VN);
     __shared__ double2 red[kWarps + 1];
@@ -587,6 +598,7 @@ __global__ void __launch_bounds__(kThreads, 4)
             sys[slot].rr = t.y;
             sys[slot].beta = beta_d;
             sys[slot].rzp[par ^ 1] = t.x;
+            if (ctl) atomicAdd(&ctl->live, 1u);
         }
     }
     const T beta = T(beta_d);
@@ -609,6 +621,18 @@ __global__ void __launch_bounds__(kThreads, 4)
             vstore(p, row, pv[k], valid);
         }
     }
+}
+
+constexpr int kLoopUnroll = 8;  // iterations per body of a step's loop
+
+// Last kernel of a step loop's body: count its iterations, and keep looping
+// while some system still iterates and the cap is not reached.
+__global__ void bs_control(StepCtl* ctl, cudaGraphConditionalHandle loop) {
+    const unsigned int it = ctl->iter + unsigned(kLoopUnroll);
+    const unsigned int live = ctl->live;
+    ctl->iter = it;
+    ctl->live = 0u;
+    cudaGraphSetConditional(loop, (live > 0u && it < ctl->cap) ? 1u : 0u);
 }
 
 // ---- host side --------------------------------------------------------------------
@@ -704,8 +728,9 @@ struct nm_solver {
     // CUDA graph of one chunk of inner iterations; valid while the lists (and
     // so every kernel argument) are unchanged
     cudaGraphExec_t chunk_exec = nullptr;
-    int32_t chunk_iters = 0;
     bool chunk_valid = false;
+    nm::StepCtl* ctl = nullptr;    // device control words of the step loop
+    nm::StepCtl* h_ctl = nullptr;  // pinned: the cap going in, the counts coming back
     int grid_spmv_inner = 0, grid_spmv_outer = 0, grid_vec = 0, grid_scalar = 0;
     // pinned staging of admission uploads: a bump allocator, reset once the
     // stream has caught up (after each step's synchronisation)
@@ -717,6 +742,7 @@ struct nm_solver {
     cudaEvent_t up_ev = nullptr;    // orders the uploads before the next kernels
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // device time of the running step
     bool in_step = false;           // between nm_solver_step_begin and _end
+    bool step_loops = false;        // the running step launched the iteration loop
     nm_solver_counters ctr{};
     ~nm_solver();
 };
@@ -733,6 +759,8 @@ nm_solver::~nm_solver() {
     cudaFreeHost(h_sblk); cudaFreeHost(h_stile);
     cudaFreeHost(h_blk); cudaFreeHost(h_tile); cudaFreeHost(h_ref); cudaFreeHost(stage);
     if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    cudaFree(ctl);
+    cudaFreeHost(h_ctl);
     if (up_ev) cudaEventDestroy(up_ev);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -880,8 +908,9 @@ int fit_grid(int cap, int64_t count) {
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(cap, count)));
 }
 
+// One iteration of every live system (the body of a step's loop).
 template <typename V, typename T>
-int launch_inner_iters(nm_solver* S, int iters) {
+int launch_inner_body(nm_solver* S, cudaGraphConditionalHandle loop) {
     cudaStream_t s = S->stream;
     const ListHdr* H = S->hdr;
     const ListHdr& h = *S->h_hdr;
@@ -896,9 +925,10 @@ int launch_inner_iters(nm_solver* S, int iters) {
     T* z = static_cast<T*>(S->z);
     T* d = static_cast<T*>(S->d);
     const T* dinv = static_cast<const T*>(S->dinv);
-    // iters is even, so the r.z parity of every chunk starts at 0
-    for (int it = 0; it < iters; ++it) {
+    for (int it = 0; it < kLoopUnroll; ++it) {
         const int par = it & 1;
+        // the last iteration of the body counts the systems that go on
+        StepCtl* ctl = it == kLoopUnroll - 1 ? S->ctl : nullptr;
         bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
                                                               S->err);
         if (g_big) bs_alpha<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
@@ -907,10 +937,11 @@ int launch_inner_iters(nm_solver* S, int iters) {
                                                 S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
                                                 par);
         if (g_big) bs_beta<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                            S->part_tile, par);
+                                                            S->part_tile, par, ctl);
         bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
-                                                 S->part_tile, z, p, par);
+                                                 S->part_tile, z, p, par, ctl);
     }
+    bs_control<<<1, 1, 0, s>>>(S->ctl, loop);
     NM_CHECK_LAUNCH();
     return NM_OK;
 }
@@ -952,6 +983,7 @@ int prepare_solver_kernels(nm_solver* S) {
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pstart<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_alpha));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_beta));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_control));
     int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
                             spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
     if (st != NM_OK) return st;
@@ -1037,6 +1069,8 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     NM_CUDA_TRY(cudaMalloc(&S->isys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->osys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->bsys, sizeof(SysRef) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMalloc(&S->ctl, sizeof(StepCtl)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_ctl, sizeof(StepCtl) * 2));
     NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 3));
     for (int2** r : {&S->sblk, &S->stile}) {
         NM_CUDA_TRY(cudaMalloc(r, sizeof(int2) * size_t(max_systems)));
@@ -1464,7 +1498,7 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
     if (!S) return fail(NM_ERR_INVALID, "nm_solver_step_begin: NULL solver");
     if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_step_begin: a step is running");
     if (iters < 0) return fail(NM_ERR_INVALID, "nm_solver_step_begin: iters must be >= 0");
-    iters = (iters + 1) & ~1;  // whole pairs (the r.z double buffer alternates)
+    iters = (iters + kLoopUnroll - 1) / kLoopUnroll * kLoopUnroll;  // whole loop bodies
     int st = NM_OK;
     auto t0 = clk::now();
     auto lap = [&t0](double& acc) {
@@ -1496,26 +1530,49 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
     }
     lap(S->ctr.s_outer);
     if (iters > 0) {
-        if (!S->chunk_valid || S->chunk_iters != iters) {
+        if (!S->chunk_valid) {
             S->ctr.graph_captures += 1;
-            // (Re)capture the chunk; update the executable graph in place when
-            // only kernel arguments changed.
+            // The step graph: a WHILE node whose body is one iteration of every
+            // live system, ended on the device by bs_control.  Rebuilt when the
+            // work lists change; the executable graph is updated in place when
+            // the driver accepts it.
             cudaGraph_t g = nullptr;
-            NM_CUDA_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
-            switch (S->inner) {
-                case NM_F64: st = launch_inner_iters<double, double>(S, iters); break;
-                case NM_F32: st = launch_inner_iters<float, float>(S, iters); break;
-                default: st = launch_inner_iters<__nv_bfloat16, float>(S, iters); break;
+            NM_CUDA_TRY(cudaGraphCreate(&g, 0));
+            cudaGraphConditionalHandle loop;
+            cudaError_t ec = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+            cudaGraphNodeParams cp = {};
+            cudaGraphNode_t node = nullptr;
+            if (ec == cudaSuccess) {
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = loop;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                ec = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
             }
-            const cudaError_t ec = cudaStreamEndCapture(S->stream, &g);
+            if (ec == cudaSuccess)
+                ec = cudaStreamBeginCaptureToGraph(S->stream, cp.conditional.phGraph_out[0], nullptr,
+                                                   nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (ec != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail(NM_ERR_CUDA, "solver step graph: %s", cudaGetErrorString(ec));
+            }
+            switch (S->inner) {
+                case NM_F64: st = launch_inner_body<double, double>(S, loop); break;
+                case NM_F32: st = launch_inner_body<float, float>(S, loop); break;
+                default: st = launch_inner_body<__nv_bfloat16, float>(S, loop); break;
+            }
+            cudaGraph_t body = nullptr;
+            ec = cudaStreamEndCapture(S->stream, &body);
             if (st != NM_OK) {
-                if (g) cudaGraphDestroy(g);
+                cudaGraphDestroy(g);
                 return st;
             }
-            if (ec != cudaSuccess)
-                return fail(NM_ERR_CUDA, "solver chunk capture failed: %s", cudaGetErrorString(ec));
+            if (ec != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail(NM_ERR_CUDA, "solver step capture failed: %s", cudaGetErrorString(ec));
+            }
             bool updated = false;
-            if (S->chunk_exec && S->chunk_iters == iters) {
+            if (S->chunk_exec) {
                 cudaGraphExecUpdateResultInfo info;
                 updated = cudaGraphExecUpdate(S->chunk_exec, g, &info) == cudaSuccess;
                 cudaGetLastError();  // an update refusal is not an error
@@ -1532,12 +1589,14 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
                 }
             }
             cudaGraphDestroy(g);
-            S->chunk_iters = iters;
             S->chunk_valid = true;
         }
         lap(S->ctr.s_capture);
+        *S->h_ctl = StepCtl{0u, 0u, unsigned(iters), 0u};
+        NM_CUDA_TRY(cudaMemcpyAsync(S->ctl, S->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice,
+                                    S->stream));
         NM_CUDA_TRY(cudaGraphLaunch(S->chunk_exec, S->stream));
-        S->ctr.inner_iterations += iters;
+        S->step_loops = true;
     }
     NM_CUDA_TRY(cudaEventRecord(S->ev1, S->stream));
     return NM_OK;
@@ -1556,7 +1615,17 @@ extern "C" int nm_solver_step_end(nm_solver* S, int32_t* n_done) {
     NM_CUDA_TRY(cudaStreamWaitEvent(S->stream, S->up_ev, 0));
     NM_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(SysState) * size_t(S->cap_sys),
                                 cudaMemcpyDeviceToHost, S->stream));
+    if (S->step_loops)
+        NM_CUDA_TRY(cudaMemcpyAsync(S->h_ctl + 1, S->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost,
+                                    S->stream));
     NM_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->step_loops) {
+        S->ctr.inner_iterations += S->h_ctl[1].iter;
+        S->ctr.last_step_iters = S->h_ctl[1].iter;
+        S->step_loops = false;
+    } else {
+        S->ctr.last_step_iters = 0;
+    }
     S->stage_used = 0;  // every staged upload has landed
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) {

@@ -104,7 +104,7 @@ def serve(requests, solver, tol: float = 1e-8, max_iter: int = 100000, chunk: in
         nxt_rows = sum(requests[i][1].nrows for i in queue[:batch])
         need = per_row * nxt_rows
         last = c["last_step_ms"] * 1e-3
-        per_it = last / max(1, solver.last_iters) if last > 0 else 0.0
+        per_it = last / max(1, c["last_step_iters"]) if last > 0 else 0.0
         if per_it <= 0:
             return chunk * 4, need
         it = int(min(64 * chunk, max(chunk, need / per_it)))

@@ -63,7 +63,6 @@ class BatchSolver:
         self.active = set()  # slots not yet finished
         self.seconds = {"admit": 0.0, "step": 0.0, "take": 0.0}  # host wall time per call kind
         self.rows_admitted = 0  # rows of all systems admitted so far
-        self.last_iters = 0     # inner iterations of the last step (rounded up to even)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -138,7 +137,8 @@ class BatchSolver:
         return out
 
     def step(self, iters: int = 8):
-        """Refinement steps + `iters` inner iterations (rounded up to even);
+        """Refinement steps + up to `iters` inner iterations (a multiple of 8;
+        the device stops early once no system iterates);
         returns the slots that finished in this step."""
         self.step_begin(iters)
         return self.step_end()
@@ -148,7 +148,6 @@ class BatchSolver:
         before step_end() (their host work overlaps the device)."""
         t0 = time.perf_counter()
         _lib.check(self.lib.nm_solver_step_begin(self._h, int(iters)), "step")
-        self.last_iters = (int(iters) + 1) & ~1
         self.seconds["step"] += time.perf_counter() - t0
 
     def step_end(self):
