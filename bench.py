@@ -632,7 +632,11 @@ def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, loc
     out = {"ms": t0.elapsed_time(t1), "stats": stats, "ctr0": c0, "ctr1": c1,
            "max_true_residual": max(errs) if errs else None, "clocks": clk.summary()}
     if with_plain:
-        pst, _ = serve.serve_plain(requests, tol=1e-8)
+        # the plain drop-in's pass time varies with host work (uploads, frees):
+        # compare against the better of two passes
+        runs = [serve.serve_plain(requests, tol=1e-8)[0] for _ in range(2)]
+        pst = max(runs, key=lambda r: r["solves_per_s"])
+        pst["passes_solves_per_s"] = [round(r["solves_per_s"], 3) for r in runs]
         out["plain"] = pst
     return out
 
@@ -676,6 +680,8 @@ def run_serve(args, rank, world, local_rank):
         "plain_fp64_drop_in": {"solves_per_s": round(plain["solves_per_s"], 3),
                                "p50_ms": round(plain["p50_ms"], 3),
                                "p99_ms": round(plain["p99_ms"], 3),
+                               "passes": plain["passes_solves_per_s"],
+                               "note": "the better of two passes",
                                "api": "kokkos_spmv.upload_csr + cg_solve_local, one request at "
                                       "a time in arrival order"},
         "ratio_vs_plain": round(solves_s / plain["solves_per_s"], 3),
@@ -717,6 +723,7 @@ def secondary(local_rank):
         "served_fp32_ir_solves_per_s": round(200 / (s["ms"] * 1e-3), 2),
         "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
         "plain_fp64_solves_per_s": round(s["plain"]["solves_per_s"], 2),
+        "plain_passes": s["plain"]["passes_solves_per_s"],
         "plain_p50_ms": round(s["plain"]["p50_ms"], 2),
         "plain_p99_ms": round(s["plain"]["p99_ms"], 2),
         "ratio_vs_plain": round(200 / (s["ms"] * 1e-3) / s["plain"]["solves_per_s"], 3),
