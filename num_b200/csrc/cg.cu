@@ -19,6 +19,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "cg.cuh"
 #include "spmv.cuh"
@@ -356,16 +358,51 @@ std::atomic<int> g_cg_persistent{1};  // nm_cg_set_persistent
 constexpr int64_t kCoopMaxRows = 262144;
 }  // namespace
 
+namespace {
+
+// Pinned host slots for the CG state copies: slabs allocated once
+// (portable pinned memory, kept until exit) and handed out per workspace, so
+// a solve on a new matrix pays no page-locking and its teardown no pinned free.
+class PinnedSlots {
+  public:
+    CgState* get() {
+        std::lock_guard<std::mutex> g(mu_);
+        if (free_.empty()) {
+            constexpr int kSlab = 256;
+            void* slab = nullptr;
+            if (cudaHostAlloc(&slab, sizeof(CgState) * kSlab, cudaHostAllocPortable) != cudaSuccess)
+                return nullptr;
+            auto* c = static_cast<CgState*>(slab);
+            for (int i = kSlab - 1; i >= 0; --i) free_.push_back(c + i);
+        }
+        CgState* out = free_.back();
+        free_.pop_back();
+        return out;
+    }
+    void put(CgState* c) {
+        if (!c) return;
+        std::lock_guard<std::mutex> g(mu_);
+        free_.push_back(c);
+    }
+
+  private:
+    std::mutex mu_;
+    std::vector<CgState*> free_;
+};
+
+PinnedSlots& pinned_slots() {
+    static PinnedSlots* s = new PinnedSlots();  // never destroyed: slots outlive statics
+    return *s;
+}
+
+}  // namespace
+
 CgWorkspace::~CgWorkspace() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
-    cudaFree(r);
-    cudaFree(p);
-    cudaFree(Ap);
-    cudaFree(partials);
-    cudaFree(st);
-    cudaFreeHost(h_in);
-    cudaFreeHost(h_out);
+    cudaFree(dmem);
+    pinned_slots().put(h_in);
+    pinned_slots().put(h_out);
 }
 
 namespace {
@@ -405,14 +442,9 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     const int64_t n = A->nrows;
     ws->n = n;
     ws->grid_vec = vec_grid(n);
-    NM_CUDA_TRY(cudaMalloc(&ws->r, sizeof(double) * size_t(n)));
-    NM_CUDA_TRY(cudaMalloc(&ws->p, sizeof(double) * size_t(n)));
-    NM_CUDA_TRY(cudaMalloc(&ws->Ap, sizeof(double) * size_t(n)));
-    NM_CUDA_TRY(cudaMalloc(&ws->st, sizeof(CgState)));
-    NM_CUDA_TRY(cudaMemset(ws->st, 0, sizeof(CgState)));
-    NM_CUDA_TRY(cudaMallocHost(&ws->h_in, sizeof(CgState)));
-    NM_CUDA_TRY(cudaMallocHost(&ws->h_out, sizeof(CgState)));
-    NM_CUDA_TRY(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
+    ws->h_in = pinned_slots().get();
+    ws->h_out = pinned_slots().get();
+    if (!ws->h_in || !ws->h_out) return fail(NM_ERR_NOMEM, "cg: no pinned host memory");
     // Load the iteration kernels and set their shared-memory attributes now
     // (lazy module loading), not during graph capture.
     cudaFuncAttributes fa;
@@ -427,6 +459,20 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     if (st != NM_OK) return st;
     ws->grid_spmv = spmv_grid(A, occ);
     ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
+    {
+        // r, p, Ap, the CTA partial sums and the state in one allocation
+        // (each part 256-byte aligned)
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t vb = up(sizeof(double) * size_t(n));
+        const size_t pb = up(sizeof(double) * size_t(ws->partials_cap));
+        NM_CUDA_TRY(cudaMalloc(&ws->dmem, 3 * vb + pb + up(sizeof(CgState))));
+        auto* base = static_cast<unsigned char*>(ws->dmem);
+        ws->r = reinterpret_cast<double*>(base);
+        ws->p = reinterpret_cast<double*>(base + vb);
+        ws->Ap = reinterpret_cast<double*>(base + 2 * vb);
+        ws->partials = reinterpret_cast<double*>(base + 3 * vb);
+        ws->st = reinterpret_cast<CgState*>(base + 3 * vb + pb);  // written by every solve
+    }
     {
         // The persistent solve runs on the same grid, every CTA resident.
         int dev = 0, coop_ok = 0, occ_c = 0;
@@ -443,7 +489,6 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
         ws->coop = coop_ok && int64_t(occ_c) * sm_count() >= ws->grid_spmv &&
                    n <= kCoopMaxRows;
     }
-    NM_CUDA_TRY(cudaMalloc(&ws->partials, sizeof(double) * size_t(ws->partials_cap)));
     ws->err = device_error_word();
     if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
     A->cg = std::move(ws);
@@ -487,6 +532,8 @@ int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* ou
         return NM_OK;
     }
     cudaGraph_t g = nullptr;
+    if (!ws->cap_stream)
+        NM_CUDA_TRY(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
     NM_CUDA_TRY(cudaStreamBeginCapture(ws->cap_stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < iters; ++i) launch_iteration(A, ws, ws->cap_stream);
     cudaError_t e = cudaStreamEndCapture(ws->cap_stream, &g);

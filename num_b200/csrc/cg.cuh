@@ -39,8 +39,9 @@ struct CgWorkspace {
     double* partials = nullptr;
     int partials_cap = 0;
     CgState* st = nullptr;
-    CgState* h_in = nullptr;    // pinned staging of the inputs
-    CgState* h_out = nullptr;   // pinned landing of the outputs
+    void* dmem = nullptr;       // one device allocation holding r, p, Ap, partials, st
+    CgState* h_in = nullptr;    // pinned staging of the inputs (a slot of a shared slab)
+    CgState* h_out = nullptr;   // pinned landing of the outputs (idem)
     int grid_spmv = 0, grid_vec = 0;
     unsigned int* err = nullptr;  // device error word (not owned)
     cudaStream_t cap_stream = nullptr;
