@@ -93,16 +93,17 @@ def serve(requests, solver, tol: float = 1e-8, max_iter: int = 100000, chunk: in
 
     def step_iters():
         # While requests wait, size the step so that its device time covers
-        # the host time of admitting the next batch (both estimated from the
-        # counters: device ms per iteration of the last step, host seconds of
-        # preparation per admitted row so far).
+        # the host time of admitting the next batch, with 1.5x headroom (both
+        # estimated: device ms per iteration of the last step, host seconds
+        # spent in admission calls per admitted row so far).
         if not queue:
             return chunk, 0.0
         c = solver.counters()
         rows_done = max(1, solver.rows_admitted)
-        per_row = c["s_admit_prep"] / rows_done if c["s_admit_prep"] > 0 else 1e-7
+        spent = solver.seconds["admit"]
+        per_row = spent / rows_done if spent > 0 else 1e-7
         nxt_rows = sum(requests[i][1].nrows for i in queue[:batch])
-        need = per_row * nxt_rows
+        need = 1.5 * per_row * nxt_rows
         last = c["last_step_ms"] * 1e-3
         per_it = last / max(1, c["last_step_iters"]) if last > 0 else 0.0
         if per_it <= 0:
