@@ -84,7 +84,7 @@ struct StepCtl {
 };
 
 
-constexpr int kTileRows = 2048;  // rows per vector-kernel tile (within one system)
+constexpr int kTileRows = 4096;  // rows per vector-kernel tile (within one system)
 
 // A system is "large" when re-reducing its block sums in every tile CTA would
 // cost more than a couple of loads per thread: its alpha and beta are then
@@ -500,8 +500,9 @@ __global__ void __launch_bounds__(kThreads, 4)
             alpha_d = pAp != 0.0 ? rz_old / pAp : 0.0;
         }
         const T alpha = T(alpha_d);
-        // two vectors of each operand per thread in flight at a time
-        constexpr int KB = IT < 2 ? IT : 2;
+        // vectors of each operand per thread in flight at a time (within 64
+        // registers): two for FP32, one for FP64
+        constexpr int KB = sizeof(T) == 4 ? (IT < 2 ? IT : 2) : 1;
 #pragma unroll
         for (int k0 = 0; k0 < IT; k0 += KB) {
             T pv[KB][VN], av[KB][VN], rv[KB][VN], dv[KB][VN], mv[KB][VN];
@@ -602,23 +603,28 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
     }
     const T beta = T(beta_d);
-    T zv[IT][VN], pv[IT][VN];
+    // four vectors of each operand per thread in flight at a time
+    constexpr int KB = IT < 4 ? IT : 4;
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-        const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
-        if (row < tl.y) {
-            vload(z, row, zv[k]);
-            vload(p, row, pv[k]);
+    for (int k0 = 0; k0 < IT; k0 += KB) {
+        T zv[KB][VN], pv[KB][VN];
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
+            if (row < tl.y) {
+                vload(z, row, zv[k]);
+                vload(p, row, pv[k]);
+            }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-        const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + k * kThreads);
-        if (row < tl.y) {
-            const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
+        for (int k = 0; k < KB; ++k) {
+            const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
+            if (row < tl.y) {
+                const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
 #pragma unroll
-            for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
-            vstore(p, row, pv[k], valid);
+                for (int e = 0; e < VN; ++e) pv[k][e] = fma(beta, pv[k][e], zv[k][e]);
+                vstore(p, row, pv[k], valid);
+            }
         }
     }
 }
