@@ -201,3 +201,27 @@ def test_large_system_scalar_path(kspmv, oracle, precision):
     S2 = _solver(precision, rows=1_000_000, nnz=6_000_000, systems=16)
     out = S2.solve([mix[0], (A, b), mix[1]], tol=1e-8, max_iter=20000, chunk=16)
     assert out[1][1]["iters"] == info["iters"] and np.array_equal(out[1][0], x)
+
+
+def test_served_stream_results_equal_alone(kspmv):
+    # Continuous batching end to end: 24 requests (2-D Laplacians and banded
+    # SPD systems) arriving by a Poisson process at 400 req/s are served with
+    # admissions overlapping running steps; every result reaches the tolerance
+    # on its true residual and carries the same bits as the same system solved
+    # alone on a fresh solver.
+    from num_b200 import serve
+    from num_b200.solver import BatchSolver
+    reqs = serve.make_requests(24, rate=400.0, seed=7, side_range=(16, 160),
+                               banded_range=(64, 8192))
+    S = BatchSolver(4_000_000, 30_000_000, 64, precision="fp32")
+    got = {}
+    stats, rec = serve.serve(reqs, S, tol=1e-8, chunk=16,
+                             check=lambda i, x, info: got.__setitem__(i, (x, info)))
+    assert stats["completed"] == len(reqs) and len(got) == len(reqs)
+    assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    for i, (t, A, b, kind) in enumerate(reqs):
+        x, info = got[i]
+        assert info["converged"] and _true_rel(A, x, b) < 1e-8, kind
+        alone = BatchSolver(4_000_000, 30_000_000, 4, precision="fp32")
+        (xa, ia), = alone.solve([(A, b)], tol=1e-8, chunk=16)
+        assert ia["iters"] == info["iters"] and np.array_equal(xa, x), kind
