@@ -285,8 +285,15 @@ def run_spmv(args, rank, world, local_rank):
         M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols,
                              precision=precision)
         batch = None
-    tuned = kspmv.tune(M, tile=args.tile, short_max=args.short_max, stages=args.stages,
-                       grid_mult=args.grid_mult)
+    if args.tile or args.short_max or args.stages or args.grid_mult >= 0:
+        tuned = kspmv.tune(M, tile=args.tile, short_max=args.short_max, stages=args.stages,
+                           grid_mult=args.grid_mult)
+        tuned["chosen_by"] = "command line"
+    else:
+        # the project's autotuner picks the partition and launch shape
+        at = kspmv.autotune(M, budget_ms=200, cache=False)
+        tuned = {k: at[k] for k in ("tile", "max_rows", "short_max", "grid_mult", "stages")}
+        tuned["chosen_by"] = f"autotune ({len(at['trials'])} candidates timed)"
     dt = torch.float64 if precision == "fp64" else torch.float32
     xd = torch.tensor(x, dtype=dt, device=dev)
     yd = torch.empty(A.nrows, dtype=dt, device=dev)
