@@ -738,6 +738,10 @@ struct nm_solver {
     nm::StepCtl* ctl = nullptr;    // device control words of the step loop
     nm::StepCtl* h_ctl = nullptr;  // pinned: the cap going in, the counts coming back
     int grid_spmv_inner = 0, grid_spmv_outer = 0, grid_vec = 0, grid_scalar = 0;
+    int64_t lists_gen = 0;   // bumped when the work-list arrays are reallocated
+    int64_t graph_gen = -1;  // lists_gen the step graph was built against
+    int graph_tiles = 0;     // tile grid of the step graph
+    bool graph_big = false;  // the step graph includes bs_alpha / bs_beta
     // pinned staging of admission uploads: a bump allocator, reset once the
     // stream has caught up (after each step's synchronisation)
     unsigned char* stage = nullptr;
@@ -781,6 +785,7 @@ size_t inner_bytes(int inner) { return inner == NM_F64 ? 8 : 4; }
 size_t inner_val_bytes(int inner) { return inner == NM_F64 ? 8 : (inner == NM_F32 ? 4 : 2); }
 
 int grow_lists(nm_solver* S, int64_t need_blk, int64_t need_tile) {
+    if (need_blk > S->cap_blk || need_tile > S->cap_tile) S->lists_gen += 1;
     if (need_blk > S->cap_blk) {
         const int64_t c = std::max<int64_t>(need_blk, 2 * S->cap_blk);
         cudaFree(S->iblk); cudaFree(S->oblk); cudaFree(S->part_blk); cudaFreeHost(S->h_blk);
@@ -868,7 +873,6 @@ int upload_lists(nm_solver* S) {
     NM_CUDA_TRY(cudaMemcpyAsync(S->stile, S->h_stile, sizeof(int2) * size_t(S->cap_sys),
                                 cudaMemcpyHostToDevice, s));
     S->lists_dirty = false;
-    S->chunk_valid = false;
     return NM_OK;
 }
 
@@ -909,6 +913,13 @@ CsrView<V> arena_view(const nm_solver* S, const void* values, const BlockDesc* l
     return M;
 }
 
+// One CTA per tile: the tile count rounded up to a power of two.
+int tile_bucket(int64_t tiles) {
+    int64_t b = 1;
+    while (b < tiles) b <<= 1;
+    return int(std::min<int64_t>(b, INT32_MAX));
+}
+
 // Grid of a persistent kernel over `count` items (at least one CTA).
 int fit_grid(int cap, int64_t count) {
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(cap, count)));
@@ -920,9 +931,14 @@ int launch_inner_body(nm_solver* S, cudaGraphConditionalHandle loop) {
     cudaStream_t s = S->stream;
     const ListHdr* H = S->hdr;
     const ListHdr& h = *S->h_hdr;
-    const int g_spmv = fit_grid(S->grid_spmv_inner, h.iblk);
-    const int g_vec = fit_grid(INT32_MAX, h.itile);  // one CTA per tile
-    const int g_big = h.bsys > 0 ? fit_grid(S->grid_scalar, h.bsys) : 0;
+    // Grids that do not follow every change of the lists (their lengths are
+    // read on the device): the persistent SpMV and scalar grids are fixed,
+    // the one-CTA-per-tile grid is the tile count rounded up to a power of
+    // two (CTAs past the count return at once), so the step graph is rebuilt
+    // only when the tile count crosses a power of two.
+    const int g_spmv = S->grid_spmv_inner;
+    const int g_vec = tile_bucket(h.itile);
+    const int g_big = h.bsys > 0 ? S->grid_scalar : 0;
     const CsrView<V> M = arena_view<V>(S, S->vin ? S->vin : S->v64, S->iblk, &H->iblk);
     constexpr size_t smem = spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>();
     T* p = static_cast<T*>(S->p);
@@ -1536,7 +1552,10 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
     }
     lap(S->ctr.s_outer);
     if (iters > 0) {
-        if (!S->chunk_valid) {
+        const bool big = S->h_hdr->bsys > 0;
+        const int tiles = tile_bucket(S->h_hdr->itile);
+        if (!S->chunk_valid || S->graph_big != big || S->graph_tiles != tiles ||
+            S->graph_gen != S->lists_gen) {
             S->ctr.graph_captures += 1;
             // The step graph: a WHILE node whose body is one iteration of every
             // live system, ended on the device by bs_control.  Rebuilt when the
@@ -1596,6 +1615,9 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
             }
             cudaGraphDestroy(g);
             S->chunk_valid = true;
+            S->graph_big = big;
+            S->graph_tiles = tiles;
+            S->graph_gen = S->lists_gen;
         }
         lap(S->ctr.s_capture);
         *S->h_ctl = StepCtl{0u, 0u, unsigned(iters), 0u};
