@@ -286,6 +286,12 @@ int nm_solver_status(const nm_solver* S, int32_t slot, int32_t* phase, nm_cg_res
 /* Copy the solution to host memory (x_host may be NULL) and free the slot. */
 int nm_solver_take(nm_solver* S, int32_t slot, double* x_host);
 
+/* nm_solver_take for `count` distinct slots at once: x_host[k] (NULL, or
+ * x_host itself NULL: discard) receives the solution of slots[k]; one stream
+ * synchronisation for all.  Not between step_begin and step_end. */
+int nm_solver_take_batch(nm_solver* S, int32_t count, const int32_t* slots,
+                         double* const* x_host);
+
 /* Solve an admitted system again (same matrix): b_host (NULL: keep b) and
  * x0_host (NULL: zero) are copied in, the iteration state is reset, and the
  * system rejoins at the next step.  Not between step_begin and step_end. */

@@ -84,6 +84,7 @@ _SIGNATURES = {
     "nm_solver_admit_batch": ([vp, i32, vp, vp, vp, vp, vp, dbl, i32, P_i32, P_i32], C.c_int),
     "nm_solver_step": ([vp, i32, P_i32], C.c_int),
     "nm_solver_step_begin": ([vp, i32], C.c_int),
+    "nm_solver_take_batch": ([vp, i32, vp, vp], C.c_int),
     "nm_solver_resolve": ([vp, i32, vp, vp], C.c_int),
     "nm_solver_stream": ([vp, C.POINTER(vp)], C.c_int),
     "nm_solver_solution": ([vp, i32, vp], C.c_int),

@@ -641,6 +641,12 @@ __global__ void bs_control(StepCtl* ctl, cudaGraphConditionalHandle loop) {
     cudaGraphSetConditional(loop, (live > 0u && it < ctl->cap) ? 1u : 0u);
 }
 
+// Marks the listed slots free (nm_solver_take_batch).
+__global__ void bs_free_slots(const int32_t* slots, int32_t count, SysState* sys) {
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+        sys[slots[k]].phase = kSysFree;
+}
+
 // ---- host side --------------------------------------------------------------------
 
 // First-fit range allocator over [0, cap).
@@ -735,6 +741,10 @@ struct nm_solver {
     // so every kernel argument) are unchanged
     cudaGraphExec_t chunk_exec = nullptr;
     bool chunk_valid = false;
+    // nm_solver_take_batch: pinned landing of the solutions, slot lists
+    double* take_stage = nullptr;
+    size_t take_cap = 0;
+    int32_t *d_slots = nullptr, *h_slots = nullptr;
     nm::StepCtl* ctl = nullptr;    // device control words of the step loop
     nm::StepCtl* h_ctl = nullptr;  // pinned: the cap going in, the counts coming back
     int grid_spmv_inner = 0, grid_spmv_outer = 0, grid_vec = 0, grid_scalar = 0;
@@ -771,6 +781,9 @@ nm_solver::~nm_solver() {
     if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
     cudaFree(ctl);
     cudaFreeHost(h_ctl);
+    cudaFreeHost(take_stage);
+    cudaFree(d_slots);
+    cudaFreeHost(h_slots);
     if (up_ev) cudaEventDestroy(up_ev);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1006,6 +1019,7 @@ int prepare_solver_kernels(nm_solver* S) {
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_alpha));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_beta));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_control));
+    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_free_slots));
     int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
                             spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
     if (st != NM_OK) return st;
@@ -1092,6 +1106,8 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     NM_CUDA_TRY(cudaMalloc(&S->osys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->bsys, sizeof(SysRef) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMalloc(&S->ctl, sizeof(StepCtl)));
+    NM_CUDA_TRY(cudaMalloc(&S->d_slots, sizeof(int32_t) * size_t(max_systems)));
+    NM_CUDA_TRY(cudaMallocHost(&S->h_slots, sizeof(int32_t) * size_t(max_systems)));
     NM_CUDA_TRY(cudaMallocHost(&S->h_ctl, sizeof(StepCtl) * 2));
     NM_CUDA_TRY(cudaMallocHost(&S->h_ref, sizeof(SysRef) * size_t(max_systems) * 3));
     for (int2** r : {&S->sblk, &S->stile}) {
@@ -1795,6 +1811,63 @@ extern "C" int nm_solver_stream(const nm_solver* S, void** stream) {
     nm::clear_error();
     if (!S || !stream) return fail(NM_ERR_INVALID, "nm_solver_stream: NULL argument");
     *stream = S->stream;
+    return NM_OK;
+}
+
+extern "C" int nm_solver_take_batch(nm_solver* S, int32_t count, const int32_t* slots,
+                                    double* const* x_host) {
+    using namespace nm;
+    clear_error();
+    if (!S || count < 0 || (count > 0 && !slots))
+        return fail(NM_ERR_INVALID, "nm_solver_take_batch: NULL argument");
+    if (S->in_step) return fail(NM_ERR_INVALID, "nm_solver_take_batch: a step is running");
+    if (count > S->cap_sys) return fail(NM_ERR_INVALID, "nm_solver_take_batch: too many slots");
+    if (count == 0) return NM_OK;
+    size_t rows = 0;
+    std::vector<char> seen(size_t(S->cap_sys), 0);
+    for (int32_t k = 0; k < count; ++k) {
+        const int32_t sl = slots[k];
+        if (sl < 0 || sl >= S->cap_sys || !S->sys[sl].used)
+            return fail(NM_ERR_INVALID, "nm_solver_take_batch: no system in slot %d", sl);
+        if (seen[size_t(sl)]) return fail(NM_ERR_INVALID, "nm_solver_take_batch: slot %d twice", sl);
+        seen[size_t(sl)] = 1;
+        rows += size_t(S->sys[sl].n);
+    }
+    if (x_host && rows > S->take_cap) {
+        const size_t cap = std::max(rows, 2 * S->take_cap);
+        cudaFreeHost(S->take_stage);
+        S->take_stage = nullptr;
+        S->take_cap = 0;
+        NM_CUDA_TRY(cudaMallocHost(&S->take_stage, sizeof(double) * cap));
+        S->take_cap = cap;
+    }
+    cudaStream_t s = S->stream;
+    size_t off = 0;
+    if (x_host) {
+        for (int32_t k = 0; k < count; ++k) {
+            const HostSys& h = S->sys[slots[k]];
+            NM_CUDA_TRY(cudaMemcpyAsync(S->take_stage + off, S->x + h.row0, sizeof(double) * size_t(h.n),
+                                        cudaMemcpyDeviceToHost, s));
+            off += size_t(h.n);
+        }
+    }
+    std::memcpy(S->h_slots, slots, sizeof(int32_t) * size_t(count));
+    NM_CUDA_TRY(cudaMemcpyAsync(S->d_slots, S->h_slots, sizeof(int32_t) * size_t(count),
+                                cudaMemcpyHostToDevice, s));
+    bs_free_slots<<<(count + 255) / 256, 256, 0, s>>>(S->d_slots, count, S->st);
+    NM_CHECK_LAUNCH();
+    NM_CUDA_TRY(cudaStreamSynchronize(s));
+    off = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        HostSys& h = S->sys[slots[k]];
+        if (x_host && x_host[k]) std::memcpy(x_host[k], S->take_stage + off, sizeof(double) * size_t(h.n));
+        off += size_t(h.n);
+        S->rows.release(h.row0, h.nrows_alloc);
+        S->nnz.release(h.z0, h.nnz_alloc);
+        if (h.phase == kSysInner || h.phase == kSysOuter) S->lists_dirty = true;
+        h = HostSys{};
+        S->h_st[slots[k]].phase = kSysFree;
+    }
     return NM_OK;
 }
 

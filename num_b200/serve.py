@@ -124,9 +124,9 @@ def serve(requests, solver, tol: float = 1e-8, max_iter: int = 100000, chunk: in
         solver.step_begin(iters)
         arrivals()
         admit_budgeted(max(budget, 1e-3))  # host preparation overlaps the step on the device
-        for slot in solver.step_end():
+        done = solver.step_end()
+        for slot, (x, info) in zip(done, solver.take_many(done)):
             i = live.pop(slot)
-            x, info = solver.take(slot)
             t_fin = time.perf_counter() - t0
             rec[i] = {"latency": t_fin - requests[i][0], "finish": t_fin, **info}
             if check is not None:

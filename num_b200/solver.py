@@ -218,6 +218,25 @@ class BatchSolver:
         _lib.check(self.lib.nm_solver_counters_get(self._h, C.byref(c)), "counters")
         return {n: getattr(c, n) for n, _ in c._fields_}
 
+    def take_many(self, slots):
+        """take() for several slots with one device synchronisation; returns
+        [(x, info)] in the order of `slots`."""
+        slots = list(slots)
+        if not slots:
+            return []
+        t0 = time.perf_counter()
+        infos = [self.status(s) for s in slots]
+        xs = [np.empty(self.n[s], np.float64) for s in slots]
+        k = len(slots)
+        arr = (C.c_int32 * k)(*slots)
+        ptrs = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
+        _lib.check(self.lib.nm_solver_take_batch(self._h, k, arr, ptrs), "take_many")
+        self.seconds["take"] += time.perf_counter() - t0
+        for s in slots:
+            self.n.pop(s, None)
+            self.active.discard(s)
+        return list(zip(xs, infos))
+
     def info(self) -> dict:
         fr, fz = C.c_int64(), C.c_int64()
         a, fs = C.c_int32(), C.c_int32()
@@ -249,6 +268,7 @@ class BatchSolver:
             self.step_begin(chunk)
             if nxt < len(systems):
                 admit()  # host preparation overlaps the step
-            for s in self.step_end():
-                out[owner.pop(s)] = self.take(s)
+            done = self.step_end()
+            for s, r in zip(done, self.take_many(done)):
+                out[owner.pop(s)] = r
         return out

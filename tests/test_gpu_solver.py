@@ -225,3 +225,27 @@ def test_served_stream_results_equal_alone(kspmv):
         alone = BatchSolver(4_000_000, 30_000_000, 4, precision="fp32")
         (xa, ia), = alone.solve([(A, b)], tol=1e-8, chunk=16)
         assert ia["iters"] == info["iters"] and np.array_equal(xa, x), kind
+
+
+def test_take_many_matches_take(kspmv):
+    # Batch retirement returns the same solutions and infos as one-by-one
+    # take(), frees the slots and rejects a slot given twice.
+    mats, _ = gen.banded_batch(12, seed=5)
+    rng = np.random.default_rng(6)
+    systems = [(A, rng.standard_normal(A.nrows)) for A in mats]
+    S1 = _solver("fp32", rows=200_000, nnz=2_000_000, systems=16)
+    S2 = _solver("fp32", rows=200_000, nnz=2_000_000, systems=16)
+    s1 = [S1.admit(A, b, tol=1e-9) for A, b in systems]
+    s2 = [S2.admit(A, b, tol=1e-9) for A, b in systems]
+    while S1.active or S2.active:
+        if S1.active:
+            S1.step(16)
+        if S2.active:
+            S2.step(16)
+    one = [S1.take(s) for s in s1]
+    with pytest.raises(ValueError):
+        S2.take_many([s2[0], s2[0]])
+    many = S2.take_many(s2)
+    for (xa, ia), (xb, ib) in zip(one, many):
+        assert ia == ib and np.array_equal(xa, xb)
+    assert S2.info()["free_slots"] == 16
