@@ -65,6 +65,8 @@ WORKLOADS = {
                 "launch", "spmv", "fp64"),
     "spmv_c3_fp32": ("4,096 banded SPD matrices n log-U[32,4096] (seed 2), FP32 SpMV of all in "
                      "one launch", "spmv", "fp32"),
+    "batch_c2_k128": ("3-D 7-point Laplacian 100^3, multi-RHS SpMV Y = A X with 128 columns, "
+                      "FP64", "batch", "fp64"),
     "cg_c1": ("2-D 5-point Laplacian 256^2, plain FP64 CG, b = A*1, x0 = 0, tol 1e-8", "cg",
               "fp64"),
     "cg_c4_fp64": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG FP64 to 1e-10",
@@ -401,6 +403,127 @@ def run_spmv(args, rank, world, local_rank):
     if world == 1 and args.workload == "spmv_c2a" and not args.no_secondary:
         line["secondary"] = secondary(local_rank)
     return line
+
+
+# ---- our arm: multi-RHS SpMV (the drop-in batch_spmv) -----------------------------------
+
+def batch_bytes(A, k):
+    """12 nnz + 4 (n+1) for the matrix, X read once (k doubles per column
+    index), Y written once (k doubles per row)."""
+    return 12 * A.nnz + 4 * (A.nrows + 1) + 8 * k * (A.ncols + A.nrows)
+
+
+def run_batch(args, rank, world, local_rank):
+    import torch
+
+    from num_b200 import _lib
+    from num_b200 import generators as gen
+    from num_b200 import kokkos_spmv as kspmv
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    k = 128
+    A = gen.laplacian_3d(100)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    g = torch.Generator(device=dev).manual_seed(1)
+    X = torch.rand((A.ncols, k), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    Y = torch.empty((A.nrows, k), dtype=torch.float64, device=dev)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    nbytes = batch_bytes(A, k)
+
+    def step():
+        st = lib.nm_batch_spmv(M._h, X.data_ptr(), Y.data_ptr(), k, s)
+        if st:
+            _lib.check(st, "nm_batch_spmv")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t0.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    total_ms = t0.elapsed_time(t1)
+    kern_avg_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    total_ms, kern_avg_ms = max_over_ranks([total_ms, kern_avg_ms], world, dev)
+    ms_per_step = total_ms / args.steps
+    # e2e: pinned X in, Y out, through kokkos_spmv.batch_spmv
+    Xh = X.cpu().pin_memory()
+    Yh = torch.empty_like(Y, device="cpu").pin_memory()
+    e_steps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        X.copy_(Xh, non_blocking=True)
+        kspmv.batch_spmv(M, X, Y)
+        Yh.copy_(Y, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = max_over_ranks([e0.elapsed_time(e1) / e_steps], world, dev)[0]
+    if rank != 0:
+        return None
+    peak, peak_src = measured_peak()
+    achieved = nbytes / (kern_avg_ms * 1e-3) / 1e9
+    config = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz, "k": k,
+              "bytes_per_step": nbytes,
+              "bytes_formula": "12*nnz + 4*(n+1) + 8*k*(ncols + nrows)",
+              "l2": "inputs larger than L2 (%.0f MB per step)" % (nbytes / 1e6),
+              "parallelism": f"replicas x{world}",
+              "api": "kokkos_spmv.batch_spmv (C ABI nm_batch_spmv), X and Y row-major"}
+    line = base_line(args, world, round(world * nbytes / (ms_per_step * 1e-3) / 1e9, 2),
+                     "GB/s", ms_per_step, precision, config)
+    line.update({
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                     "traffic": None, "kernel": "nm::batch_spmv_kernel",
+                     "kernel_avg_us": round(kern_avg_ms * 1e3, 3),
+                     "reference_formula_gbs": round(
+                         (12 * A.nnz + 8 * k * A.nrows + 8 * A.nrows) / (kern_avg_ms * 1e-3) / 1e9, 1)},
+        "e2e": {"value": round(nbytes / (e_ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": int(Xh.numel() * 8), "d2h_bytes_per_step": int(Yh.numel() * 8),
+                "ms_per_step": round(e_ms, 3),
+                "api": "kokkos_spmv.batch_spmv with pinned X / Y copies"},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_batch(A, k, budget_s=args.cpu_seconds)
+    return line
+
+
+def cpu_baseline_batch(A, k, budget_s=10.0):
+    from oracle import oracle
+    L = oracle.lib()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    X = np.random.default_rng(1).uniform(-1, 1, (A.ncols, k))
+    Y = np.empty((A.nrows, k))
+    rp, ci, v = (np.ascontiguousarray(a) for a in (A.row_ptr, A.col_idx, A.values))
+    run = lambda: L.or_batch_spmv_f64(A.nrows, k, rp.ctypes.data, ci.ctypes.data,
+                                      v.ctypes.data, X.ctypes.data, Y.ctypes.data)
+    run()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end and len(times) < 100:
+        t = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t)
+    med = statistics.median(times)
+    return {"value": round(batch_bytes(A, k) / med / 1e9, 3), "unit": "GB/s", "cores": threads,
+            "kind": "port",
+            "sample": f"full product, {len(times)} runs, median {med * 1e3:.1f} ms; "
+                      "oracle/oracle.c or_batch_spmv_f64 (OpenMP rows, serial per (row, column))"}
 
 
 # ---- our arm: plain CG (the drop-in cg_solve_local) ------------------------------------
@@ -888,6 +1011,13 @@ def run_reference(args, rank, world):
                   f"SpMV), or_spmv_*_omp on {threads} threads ({note})")
         cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz}
         ms_step = el / args.steps * 1e3
+    elif kind == "batch":
+        from num_b200 import generators as gen
+        A = gen.laplacian_3d(100)
+        cb = cpu_baseline_batch(A, 128, budget_s=min(60.0, 2.0 * (args.steps + args.warmup)))
+        val, unit, sample = cb["value"], "GB/s", cb["sample"] + f" ({note})"
+        cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz, "k": 128}
+        ms_step = batch_bytes(A, 128) / (val * 1e9) * 1e3
     elif kind in ("cg", "engine"):
         from num_b200 import generators as gen
         if kind == "cg":
@@ -923,7 +1053,7 @@ def run_reference(args, rank, world):
     }
 
 
-DEFAULT_STEPS = {"spmv": 2000, "cg": 50, "engine": 5, "serve": 3}
+DEFAULT_STEPS = {"spmv": 2000, "batch": 100, "cg": 50, "engine": 5, "serve": 3}
 
 
 def main():
@@ -973,7 +1103,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run = {"spmv": run_spmv, "cg": run_cg, "engine": run_engine, "serve": run_serve}[kind]
+        run = {"spmv": run_spmv, "batch": run_batch, "cg": run_cg, "engine": run_engine,
+               "serve": run_serve}[kind]
         line = run(args, rank, world, local_rank)
     finally:
         if world > 1:

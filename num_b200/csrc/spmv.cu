@@ -95,16 +95,17 @@ int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
 // Multi-RHS SpMV  Y(nrows,k) = A * X(ncols,k), row-major.
 //
 // A group of TPR = 2^tpr_log2 consecutive lanes owns one row; lane g of the
-// group owns the columns g*VEC + m*TPR*VEC (m < MCH) of the current column
-// pass, VEC = 2 with 16-byte loads when k is even.  Each (row, column) sum
+// group owns the columns g*VEC + m*TPR*VEC (m < CH) of the current column
+// pass, VEC = 2 with 16-byte loads when k is even, CH sized to k at launch.  Each (row, column) sum
 // runs serially in CSR order with unfused multiply/add, i.e. exactly the
 // reference's per-(i,b) loop (src/batch_spmv_kernel.hpp:95-102).  The
 // matrix entries of a row are read once per column pass and broadcast to the
 // group; X rows are read as contiguous segments (coalesced).
 // ---------------------------------------------------------------------------
-constexpr int kBatchChunks = 4;
+constexpr int kBatchChunks = 4;  // most column chunks per lane in one pass
+constexpr int kBatchNz = 4;      // nonzeros whose X rows are loaded together
 
-template <int VEC>
+template <int VEC, int CH>
 __global__ void __launch_bounds__(kThreads)
     batch_spmv_kernel(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                       const double* __restrict__ vals, int32_t nrows, int32_t k, int tpr_log2,
@@ -115,32 +116,53 @@ __global__ void __launch_bounds__(kThreads)
     const int g = static_cast<int>(gtid & (tpr - 1));
     if (row >= nrows) return;
     const int32_t s0 = rp[row], s1 = rp[row + 1];
-    const int pass_cols = tpr * VEC * kBatchChunks;
+    const int pass_cols = tpr * VEC * CH;
     for (int c0 = 0; c0 < k; c0 += pass_cols) {
-        double acc[kBatchChunks][VEC];
+        double acc[CH][VEC];
 #pragma unroll
-        for (int m = 0; m < kBatchChunks; ++m)
+        for (int m = 0; m < CH; ++m)
 #pragma unroll
             for (int e = 0; e < VEC; ++e) acc[m][e] = 0.0;
-        for (int32_t j = s0; j < s1; ++j) {
-            const double v = __ldg(vals + j);
-            const int64_t xrow = int64_t(__ldg(ci + j)) * k;
+        // kBatchNz nonzeros at a time: their columns and values first, then
+        // all their X row segments in flight together, then the products
+        // added in CSR order
+        for (int32_t j0 = s0; j0 < s1; j0 += kBatchNz) {
+            int64_t xr[kBatchNz];
+            double v[kBatchNz];
 #pragma unroll
-            for (int m = 0; m < kBatchChunks; ++m) {
-                const int c = c0 + (m * tpr + g) * VEC;
-                if (c < k) {
-                    if (VEC == 2) {
-                        const double2 xv = __ldg(reinterpret_cast<const double2*>(X + xrow + c));
-                        acc[m][0] = add_rn(acc[m][0], mul_rn(v, xv.x));
-                        acc[m][VEC - 1] = add_rn(acc[m][VEC - 1], mul_rn(v, xv.y));
-                    } else {
-                        acc[m][0] = add_rn(acc[m][0], mul_rn(v, __ldg(X + xrow + c)));
+            for (int q = 0; q < kBatchNz; ++q) {
+                const bool in = j0 + q < s1;
+                xr[q] = in ? int64_t(__ldg(ci + j0 + q)) * k : 0;
+                v[q] = in ? __ldg(vals + j0 + q) : 0.0;
+            }
+            double xv[kBatchNz][CH][VEC];
+#pragma unroll
+            for (int q = 0; q < kBatchNz; ++q)
+#pragma unroll
+                for (int m = 0; m < CH; ++m) {
+                    const int c = c0 + (m * tpr + g) * VEC;
+                    if (j0 + q < s1 && c < k) {
+                        if (VEC == 2) {
+                            const double2 t = __ldg(reinterpret_cast<const double2*>(X + xr[q] + c));
+                            xv[q][m][0] = t.x;
+                            xv[q][m][VEC - 1] = t.y;
+                        } else {
+                            xv[q][m][0] = __ldg(X + xr[q] + c);
+                        }
                     }
                 }
-            }
+#pragma unroll
+            for (int q = 0; q < kBatchNz; ++q)
+                if (j0 + q < s1) {
+#pragma unroll
+                    for (int m = 0; m < CH; ++m)
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e)
+                            acc[m][e] = add_rn(acc[m][e], mul_rn(v[q], xv[q][m][e]));
+                }
         }
 #pragma unroll
-        for (int m = 0; m < kBatchChunks; ++m) {
+        for (int m = 0; m < CH; ++m) {
             const int c = c0 + (m * tpr + g) * VEC;
             if (c < k) {
                 if (VEC == 2) {
@@ -154,6 +176,22 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+template <int VEC, int CH>
+static void launch_batch_t(const nm_csr* A, const double* X, double* Y, int32_t k, int tpr_log2,
+                           int grid, cudaStream_t s) {
+    batch_spmv_kernel<VEC, CH><<<grid, kThreads, 0, s>>>(
+        A->d_row_ptr, A->d_col_idx, static_cast<const double*>(A->d_values), A->nrows, k,
+        tpr_log2, X, Y);
+}
+
+template <int VEC>
+static void launch_batch_v(const nm_csr* A, const double* X, double* Y, int32_t k, int tpr_log2,
+                           int ch, int grid, cudaStream_t s) {
+    if (ch >= 4) launch_batch_t<VEC, 4>(A, X, Y, k, tpr_log2, grid, s);
+    else if (ch == 2 || ch == 3) launch_batch_t<VEC, 2>(A, X, Y, k, tpr_log2, grid, s);
+    else launch_batch_t<VEC, 1>(A, X, Y, k, tpr_log2, grid, s);
+}
+
 static int launch_batch(const nm_csr* A, const double* X, double* Y, int32_t k, cudaStream_t s) {
     const bool vec2 = (k % 2 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0) &&
                       (reinterpret_cast<uintptr_t>(Y) % 16 == 0);
@@ -161,17 +199,13 @@ static int launch_batch(const nm_csr* A, const double* X, double* Y, int32_t k, 
     const int groups = (k + vec - 1) / vec;  // lane-columns needed for one pass
     int tpr_log2 = 0;
     while ((1 << tpr_log2) < groups && tpr_log2 < 5) ++tpr_log2;
+    // column chunks per lane: enough for k in one pass, at most kBatchChunks
+    const int ch = std::min(kBatchChunks, (groups + (1 << tpr_log2) - 1) >> tpr_log2);
     const int64_t threads = int64_t(A->nrows) << tpr_log2;
     const int64_t grid = (threads + kThreads - 1) / kThreads;
     if (grid > INT32_MAX) return fail(NM_ERR_INVALID, "batch_spmv: problem too large");
-    if (vec2)
-        batch_spmv_kernel<2><<<static_cast<int>(grid), kThreads, 0, s>>>(
-            A->d_row_ptr, A->d_col_idx, static_cast<const double*>(A->d_values), A->nrows, k,
-            tpr_log2, X, Y);
-    else
-        batch_spmv_kernel<1><<<static_cast<int>(grid), kThreads, 0, s>>>(
-            A->d_row_ptr, A->d_col_idx, static_cast<const double*>(A->d_values), A->nrows, k,
-            tpr_log2, X, Y);
+    if (vec2) launch_batch_v<2>(A, X, Y, k, tpr_log2, ch, static_cast<int>(grid), s);
+    else launch_batch_v<1>(A, X, Y, k, tpr_log2, ch, static_cast<int>(grid), s);
     NM_CHECK_LAUNCH();
     return NM_OK;
 }
