@@ -13,6 +13,8 @@ Other workloads (--workload):
   spmv_c2a_fp32, spmv_c2b[_fp32], spmv_c1     one SpMV per step
   spmv_c3[_fp32]    4,096 banded SPD matrices (n log-uniform in [32, 4096],
                     seed 2) multiplied in one launch per step
+  batch_c2_k128     one multi-RHS SpMV Y = A X per step (100^3 Laplacian,
+                    128 right-hand sides), the drop-in batch_spmv
   cg_c1             one plain FP64 CG solve per step (256^2 Laplacian,
                     b = A 1, x0 = 0, tol 1e-8), the drop-in cg_solve_local
   cg_c4_fp64 / cg_c4_fp32 / cg_c4_bf16
