@@ -7,7 +7,8 @@ Default workload (one step = one FP64 CSR SpMV, y = A x):
   Algorithmic bytes per SpMV = 12 nnz + 4 (n + 1) + 8 n (x) + 8 n (y)
   = 424.14 MB, larger than the 126 MB L2, so no flush is needed between steps.
   The default line also carries a `secondary` object: plain FP64 CG solves/s
-  on the 256^2 Laplacian and a served-CG sample (see serve_c5).
+  on the 256^2 Laplacian, the 160^3 matrix setup time (host build + upload
+  against on-device assembly) and a served-CG sample (see serve_c5).
 
 Other workloads (--workload):
   spmv_c2a_fp32, spmv_c2b[_fp32], spmv_c1     one SpMV per step
@@ -836,6 +837,37 @@ def run_serve(args, rank, world, local_rank):
     return line
 
 
+def setup_c2a_measure(dev):
+    """Setup of the 160^3 Laplacian handle, wall clock, the better of two runs:
+    host generator + upload_csr (host arrays, validation, host-to-device copy,
+    partition) against kokkos_spmv.laplacian (assembly on the device, row_ptr
+    and columns read back for the partition)."""
+    import torch
+
+    from num_b200 import generators as gen
+    from num_b200 import kokkos_spmv as k
+    gen_s, up_s, dev_s = [], [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        A = gen.laplacian_3d(160)
+        t1 = time.perf_counter()
+        M = k.upload_csr(*A.astuple())
+        torch.cuda.synchronize(dev)
+        t2 = time.perf_counter()
+        gen_s.append(t1 - t0)
+        up_s.append(t2 - t1)
+        del M, A
+        t0 = time.perf_counter()
+        M = k.laplacian(3, 160)
+        torch.cuda.synchronize(dev)
+        dev_s.append(time.perf_counter() - t0)
+        del M
+    host = min(g + u for g, u in zip(gen_s, up_s))
+    return {"host_generate_s": round(min(gen_s), 4), "host_upload_s": round(min(up_s), 4),
+            "device_laplacian_s": round(min(dev_s), 4), "speedup": round(host / min(dev_s), 2),
+            "api": "generators.laplacian_3d + kokkos_spmv.upload_csr vs kokkos_spmv.laplacian"}
+
+
 def secondary(local_rank):
     """Short CG and serving numbers for the default line."""
     import torch
@@ -848,6 +880,7 @@ def secondary(local_rank):
                                "us_per_iteration": round(r["ms"] * 1e3 / r["iters"], 3),
                                "iters": r["info"]["iters"], "residual": r["info"]["residual"],
                                "e2e_solves_per_s": round(1e3 / r["e2e_ms"], 2)}
+    out["setup_c2a"] = setup_c2a_measure(dev)
     requests = serve.make_requests(200, rate=0.0, seed=4)
     s = serve_measure(dev, requests, 1, 1, 64e9)
     st = s["stats"][0]

@@ -101,6 +101,22 @@ int nm_csr_create_batched(int32_t count, const int32_t* nrows, const int32_t* nc
                           const int32_t* row_ptr, const int32_t* col_idx,
                           const void* values, int dtype, nm_csr** out);
 
+/* The 5-point 2-D (dim 2; values 4 / -1) or 7-point 3-D (dim 3; 6 / -1)
+ * Dirichlet Laplacian on an L^dim grid, x fastest, assembled on the device:
+ * the same arrays as python/matrix_generators.py make_laplacian_2d (:16-37)
+ * and make_laplacian_3d_fast (:68-80) followed by upload_csr
+ * (src/bindings.cpp:97-123), without building them on the host or copying
+ * them over PCIe (row_ptr and col_idx are read back once for the row-block
+ * partition).  Values are stored as `dtype`.  dim other than 2 / 3, L <= 0,
+ * or L^dim rows / nonzeros beyond the int32 offsets return NM_ERR_INVALID. */
+int nm_csr_laplacian(int32_t dim, int32_t L, int dtype, nm_csr** out);
+
+/* Copies the device arrays back to host buffers: row_ptr[nrows+1],
+ * col_idx[nnz], values[nnz] in the stored dtype (many-matrix handles: the
+ * block-diagonal matrix with global column indices).  Addition: the
+ * reference's CrsMatrix has no read-back. */
+int nm_csr_export(const nm_csr* A, int32_t* row_ptr, int32_t* col_idx, void* values);
+
 /* Frees the device copy (handle destructor). */
 int nm_csr_destroy(nm_csr* A);
 

@@ -60,6 +60,8 @@ _SIGNATURES = {
     "nm_csr_create": ([vp, vp, vp, C.c_int, i32, i32, C.POINTER(vp)], C.c_int),
     "nm_csr_create_batched": ([i32, vp, vp, vp, vp, vp, C.c_int, C.POINTER(vp)], C.c_int),
     "nm_csr_destroy": ([vp], C.c_int),
+    "nm_csr_laplacian": ([i32, i32, C.c_int, C.POINTER(vp)], C.c_int),
+    "nm_csr_export": ([vp, vp, vp, vp], C.c_int),
     "nm_csr_info": ([vp, P_i32, P_i32, P_i32, P_i32, P_i32], C.c_int),
     "nm_csr_set_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
     "nm_csr_get_tuning": ([vp, C.POINTER(Tuning)], C.c_int),

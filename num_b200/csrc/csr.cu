@@ -348,6 +348,79 @@ extern "C" int nm_csr_create_batched(int32_t count, const int32_t* nrows, const 
     return nm::finish_create(A, grp.data(), gci.data(), values, out);
 }
 
+extern "C" int nm_csr_laplacian(int32_t dim, int32_t L, int dtype, nm_csr** out) {
+    nm::clear_error();
+    if (!out) return fail(NM_ERR_INVALID, "nm_csr_laplacian: out is NULL");
+    *out = nullptr;
+    if (dim != 2 && dim != 3)
+        return fail(NM_ERR_INVALID, "nm_csr_laplacian: dim must be 2 or 3 (got %d)", dim);
+    if (L <= 0) return fail(NM_ERR_INVALID, "CrsMatrixHandle: non-positive dimensions");
+    const size_t es = nm::dtype_size(dtype);
+    if (es == 0) return fail(NM_ERR_TYPE, "nm_csr_laplacian: unknown dtype %d", dtype);
+    // L^dim rows and their nonzeros must fit the int32 offsets (checked in
+    // 64 bits; L above 46,341 / 1,291 already overflows the rows).
+    if ((dim == 2 && L > 46341) || (dim == 3 && L > 1291))
+        return fail(NM_ERR_INVALID, "nm_csr_laplacian: L = %d exceeds the int32 row range", L);
+    const int64_t n = dim == 2 ? int64_t(L) * L : int64_t(L) * L * L;
+    const int64_t nnz = nm::stencil_nnz(dim, L);
+    if (n > INT32_MAX || nnz > INT32_MAX - 16384)
+        return fail(NM_ERR_INVALID,
+                    "nm_csr_laplacian: L = %d gives %lld rows / %lld nonzeros, beyond the int32 "
+                    "offset range", L, (long long)n, (long long)nnz);
+    auto* A = new nm_csr();
+    cudaGetDevice(&A->device);
+    A->nrows = A->ncols = static_cast<int32_t>(n);
+    A->nnz = static_cast<int32_t>(nnz);
+    A->dtype = dtype;
+    A->tune = nm_tuning{0, 0, 0, 0, 0};
+    nm::normalise_tuning(A->tune);
+    auto build = [&]() -> int {
+        // Same allocation and padding as an uploaded matrix.
+        const int64_t nnz_pad = ((nnz + 7) & ~int64_t(7)) + 8;
+        const int64_t rp_len = n + 1 + 8;
+        NM_CUDA_TRY(cudaMalloc(&A->d_row_ptr, sizeof(int32_t) * size_t(rp_len)));
+        NM_CUDA_TRY(cudaMalloc(&A->d_col_idx, sizeof(int32_t) * size_t(nnz_pad)));
+        NM_CUDA_TRY(cudaMalloc(&A->d_values, es * size_t(nnz_pad)));
+        NM_CUDA_TRY(cudaMemset(A->d_col_idx + nnz, 0, sizeof(int32_t) * size_t(nnz_pad - nnz)));
+        NM_CUDA_TRY(cudaMemset(static_cast<char*>(A->d_values) + es * size_t(nnz), 0,
+                               es * size_t(nnz_pad - nnz)));
+        int st = nm::launch_laplacian(dim, L, dtype, A->d_row_ptr, rp_len, A->d_col_idx,
+                                      A->d_values, nullptr);
+        if (st != NM_OK) return st;
+        // The row-block partition is built on the host from row_ptr and the
+        // columns (as for an uploaded matrix): read them back once.
+        A->h_row_ptr.resize(size_t(n) + 1);
+        A->h_col_idx.resize(size_t(nnz));
+        NM_CUDA_TRY(cudaMemcpy(A->h_row_ptr.data(), A->d_row_ptr, sizeof(int32_t) * size_t(n + 1),
+                               cudaMemcpyDeviceToHost));
+        NM_CUDA_TRY(cudaMemcpy(A->h_col_idx.data(), A->d_col_idx, sizeof(int32_t) * size_t(nnz),
+                               cudaMemcpyDeviceToHost));
+        return nm::rebuild_blocks(A);
+    };
+    const int st = build();
+    if (st != NM_OK) {
+        delete A;
+        return st;
+    }
+    *out = A;
+    return NM_OK;
+}
+
+extern "C" int nm_csr_export(const nm_csr* A, int32_t* row_ptr, int32_t* col_idx, void* values) {
+    nm::clear_error();
+    if (!A || !row_ptr || (A->nnz > 0 && (!col_idx || !values)))
+        return fail(NM_ERR_INVALID, "nm_csr_export: NULL argument");
+    NM_CUDA_TRY(cudaMemcpy(row_ptr, A->d_row_ptr, sizeof(int32_t) * (size_t(A->nrows) + 1),
+                           cudaMemcpyDeviceToHost));
+    if (A->nnz > 0) {
+        NM_CUDA_TRY(cudaMemcpy(col_idx, A->d_col_idx, sizeof(int32_t) * size_t(A->nnz),
+                               cudaMemcpyDeviceToHost));
+        NM_CUDA_TRY(cudaMemcpy(values, A->d_values, nm::dtype_size(A->dtype) * size_t(A->nnz),
+                               cudaMemcpyDeviceToHost));
+    }
+    return NM_OK;
+}
+
 extern "C" int nm_csr_destroy(nm_csr* A) {
     nm::clear_error();
     delete A;

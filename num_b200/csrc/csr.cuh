@@ -118,4 +118,10 @@ size_t spmv_smem_for(int dtype, int tile, int stages);
 int rebuild_blocks(nm_csr* A);
 // Drops A's cached CG workspace (its graphs hold the current descriptors).
 void reset_cg(nm_csr* A);
+// Nonzeros of the Laplacian on an L^dim grid (dim 2: 5-point, dim 3: 7-point).
+int64_t stencil_nnz(int dim, int32_t L);
+// Writes that Laplacian's row_ptr (rp_len entries, those past the last row =
+// nnz), col_idx and values (dtype) into device arrays on `stream` (gen.cu).
+int launch_laplacian(int dim, int32_t L, int dtype, int32_t* rp, int64_t rp_len, int32_t* ci,
+                     void* val, cudaStream_t stream);
 }  // namespace nm

@@ -35,7 +35,7 @@ except ImportError:  # pragma: no cover
 __all__ = [
     "init", "finalize", "rank", "size", "barrier", "CrsMatrix", "DistCrsMatrix", "upload_csr",
     "upload_csr_batched", "distribute_csr", "spmv", "batch_spmv", "dist_spmv", "cg_solve",
-    "cg_solve_local", "tune", "tuning", "autotune", "row_blocks",
+    "cg_solve_local", "tune", "tuning", "autotune", "row_blocks", "laplacian", "download_csr",
 ]
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
@@ -220,6 +220,34 @@ def upload_csr(rowptr, colind, values, nrows: int, ncols: int, *, precision: str
     _lib.check(_lib.load().nm_csr_create(rowptr.ctypes.data, colind.ctypes.data, vals.ctypes.data,
                                          dt, nrows, ncols, C.byref(out)), "upload_csr")
     return CrsMatrix(out.value)
+
+
+def laplacian(dim: int, L: int, *, precision: str = "fp64") -> CrsMatrix:
+    """The Dirichlet Laplacian on an L^dim grid (dim 2: 5-point, 4 / -1;
+    dim 3: 7-point, 6 / -1; x fastest) assembled on the GPU (addition).
+
+    Same matrix as upload_csr of the reference generators
+    make_laplacian_2d(L) / make_laplacian_3d_fast(L)
+    (python/matrix_generators.py:16-37, :68-80), without the host build and
+    the host-to-device copy."""
+    if precision not in _PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}, got {precision!r}")
+    out = C.c_void_p()
+    _lib.check(_lib.load().nm_csr_laplacian(int(dim), int(L), _PRECISIONS[precision],
+                                            C.byref(out)), "laplacian")
+    return CrsMatrix(out.value)
+
+
+def download_csr(A: CrsMatrix):
+    """(rowptr int32, colind int32, values) copied back from the device
+    (addition); values in the stored precision (bf16 as uint16 bits)."""
+    dt = {_lib.NM_F64: np.float64, _lib.NM_F32: np.float32, _lib.NM_BF16: np.uint16}[A._dtype]
+    rp = np.empty(A.nrows + 1, np.int32)
+    ci = np.empty(max(A.nnz, 1), np.int32)
+    v = np.empty(max(A.nnz, 1), dt)
+    _lib.check(_lib.load().nm_csr_export(A._h, rp.ctypes.data, ci.ctypes.data, v.ctypes.data),
+               "download_csr")
+    return rp, ci[: A.nnz], v[: A.nnz]
 
 
 def upload_csr_batched(matrices, *, precision: str = "fp64"):

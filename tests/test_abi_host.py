@@ -138,6 +138,19 @@ def test_create_validation_errors_before_device_work(nmlib):
         _lib.check(st)
 
 
+@pytest.mark.parametrize("dim,L,what", [(4, 8, b"dim must be"), (2, 0, b"non-positive"),
+                                        (3, -1, b"non-positive"), (3, 700, b"int32 offset"),
+                                        (2, 50000, b"int32 row")])
+def test_laplacian_rejects_bad_sizes_before_device_work(nmlib, dim, L, what):
+    """nm_csr_laplacian checks dim and L (rows and nonzeros within the int32
+    offsets: 700^3 gives 2.4e9 nonzeros) on the host."""
+    from num_b200 import _lib
+    out = C.c_void_p()
+    assert nmlib.nm_csr_laplacian(dim, L, 0, C.byref(out)) == _lib.NM_ERR_INVALID
+    assert what in nmlib.nm_last_error() and not out.value
+    assert nmlib.nm_csr_laplacian(3, 4, 9, C.byref(out)) == _lib.NM_ERR_TYPE
+
+
 def test_python_module_errors_on_host(nmlib):
     """upload_csr argument checking mirrors the nanobind signature: wrong
     dtype -> TypeError, non-positive dims / short arrays -> ValueError."""
