@@ -7,6 +7,7 @@
 // arrays.  Each row's offset is a closed-form count of the nonzeros before
 // it, so one thread per row writes its row_ptr entry, its columns and its
 // values with no scan, and the matrix never crosses PCIe on the way in.
+// HBM-bound: 4 (n + 1) + (4 + value bytes) nnz written, nothing read.
 #include "csr.cuh"
 
 #include <algorithm>
@@ -43,37 +44,62 @@ int64_t stencil_nnz(int dim, int32_t L) {
 
 namespace {
 
-// One thread per row_ptr entry (n + 1 + padding): entries past row n - 1 get
-// nnz; rows write their nonzeros in ascending column order.
+// Rows in CTA-sized groups: each thread writes its row's row_ptr entry and
+// stages the row's nonzeros in shared memory at their offset within the
+// group; the CTA then writes the group's contiguous column / value range with
+// consecutive threads on consecutive elements (full-sector stores), and CTA 0
+// fills the row_ptr padding past row n - 1 with nnz.
+constexpr int kGenRows = 256;
+constexpr int kGenMaxNz = 7;  // nonzeros of a 7-point row
+
 template <typename V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kGenRows)
     laplacian_kernel(int dim, uint32_t L, uint32_t n, int64_t rp_len, int32_t* __restrict__ rp,
                      int32_t* __restrict__ ci, V* __restrict__ val, V diag, V off) {
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    __shared__ int32_t s_ci[kGenRows * kGenMaxNz];
+    __shared__ V s_v[kGenRows * kGenMaxNz];
     const uint32_t LL = L * L;
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < rp_len; t += stride) {
-        const uint32_t i = t < n ? uint32_t(t) : n;
-        int64_t j = stencil_before(dim, L, n, i);
-        rp[t] = static_cast<int32_t>(j);
-        if (t >= n) continue;
-        const uint32_t x = i % L;
-        const uint32_t y = dim == 2 ? i / L : (i / L) % L;
-        const uint32_t z = dim == 2 ? 0 : i / LL;
-        if (dim == 3 && z > 0) { ci[j] = int32_t(i - LL); val[j] = off; ++j; }
-        if (y > 0) { ci[j] = int32_t(i - L); val[j] = off; ++j; }
-        if (x > 0) { ci[j] = int32_t(i - 1); val[j] = off; ++j; }
-        ci[j] = int32_t(i); val[j] = diag; ++j;
-        if (x + 1 < L) { ci[j] = int32_t(i + 1); val[j] = off; ++j; }
-        if (y + 1 < L) { ci[j] = int32_t(i + L); val[j] = off; ++j; }
-        if (dim == 3 && z + 1 < L) { ci[j] = int32_t(i + LL); val[j] = off; }
+    const int64_t groups = (int64_t(n) + kGenRows - 1) / kGenRows;
+    for (int64_t g = blockIdx.x; g < groups; g += gridDim.x) {
+        const uint32_t r0 = uint32_t(g * kGenRows);
+        const uint32_t r1 = n - r0 < uint32_t(kGenRows) ? n : r0 + kGenRows;
+        const int64_t base = stencil_before(dim, L, n, r0);
+        const uint32_t i = r0 + threadIdx.x;
+        if (i < r1) {
+            const int64_t j0 = stencil_before(dim, L, n, i);
+            rp[i] = static_cast<int32_t>(j0);
+            int k = static_cast<int>(j0 - base);
+            const uint32_t x = i % L;
+            const uint32_t y = dim == 2 ? i / L : (i / L) % L;
+            const uint32_t z = dim == 2 ? 0 : i / LL;
+            if (dim == 3 && z > 0) { s_ci[k] = int32_t(i - LL); s_v[k] = off; ++k; }
+            if (y > 0) { s_ci[k] = int32_t(i - L); s_v[k] = off; ++k; }
+            if (x > 0) { s_ci[k] = int32_t(i - 1); s_v[k] = off; ++k; }
+            s_ci[k] = int32_t(i); s_v[k] = diag; ++k;
+            if (x + 1 < L) { s_ci[k] = int32_t(i + 1); s_v[k] = off; ++k; }
+            if (y + 1 < L) { s_ci[k] = int32_t(i + L); s_v[k] = off; ++k; }
+            if (dim == 3 && z + 1 < L) { s_ci[k] = int32_t(i + LL); s_v[k] = off; }
+        }
+        __syncthreads();
+        const int cnt = static_cast<int>(stencil_before(dim, L, n, r1) - base);
+        for (int e = threadIdx.x; e < cnt; e += kGenRows) {
+            ci[base + e] = s_ci[e];
+            val[base + e] = s_v[e];
+        }
+        __syncthreads();
     }
+    if (blockIdx.x == 0 && int64_t(n) + threadIdx.x < rp_len)
+        rp[int64_t(n) + threadIdx.x] = static_cast<int32_t>(stencil_before(dim, L, n, n));
 }
 
 template <typename V>
 int launch_t(int dim, int32_t L, int32_t n, int64_t rp_len, int32_t* rp, int32_t* ci, void* val,
              V diag, V off, cudaStream_t s) {
-    const int64_t blocks = std::min<int64_t>((rp_len + 255) / 256, int64_t(sm_count()) * 16);
-    laplacian_kernel<V><<<static_cast<int>(blocks), 256, 0, s>>>(
+    if (rp_len < int64_t(n) + 1 || rp_len - n > kGenRows)
+        return fail(NM_ERR_INVALID, "laplacian: row_ptr length %lld for %d rows", (long long)rp_len, n);
+    const int64_t blocks =
+        std::min<int64_t>((int64_t(n) + kGenRows - 1) / kGenRows, int64_t(sm_count()) * 8);
+    laplacian_kernel<V><<<static_cast<int>(blocks), kGenRows, 0, s>>>(
         dim, uint32_t(L), uint32_t(n), rp_len, rp, ci, static_cast<V*>(val), diag, off);
     NM_CHECK_LAUNCH();
     return NM_OK;

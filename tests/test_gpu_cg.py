@@ -176,7 +176,7 @@ def test_batch_identity_columns(kspmv):
     assert np.array_equal(Y.cpu().numpy(), A.to_scipy().toarray())
 
 
-@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 31, 32, 33, 64, 100, 300])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 31, 32, 33, 64, 100, 128, 257, 300])
 def test_batch_bit_exact(kspmv, oracle, k):
     A = gen.power_law(5000, seed=k)
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
@@ -184,6 +184,18 @@ def test_batch_bit_exact(kspmv, oracle, k):
     Y = torch.empty(A.nrows, k, dtype=torch.float64, device="cuda")
     kspmv.batch_spmv(M, _dev(X), Y)
     assert np.array_equal(Y.cpu().numpy(), oracle.batch_spmv(A.row_ptr, A.col_idx, A.values, X))
+
+
+def test_batch_laplacian_k128_bit_exact(kspmv, oracle):
+    # 7-nonzero rows, one warp per row, X rows shared by neighbouring rows
+    A = gen.laplacian_3d(24)
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    X = np.random.default_rng(128).uniform(-1, 1, (A.ncols, 128))
+    Y = torch.empty(A.nrows, 128, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        kspmv.batch_spmv(M, _dev(X), Y)
+        assert np.array_equal(Y.cpu().numpy(),
+                              oracle.batch_spmv(A.row_ptr, A.col_idx, A.values, X))
 
 
 def test_batch_errors(kspmv):
