@@ -167,12 +167,13 @@ __global__ void __launch_bounds__(kThreads)
 //   B  x, r update and r.r over "virtual CTAs" v = blockIdx.x, + gridDim.x,
 //      ... < grid_vec of 256 threads, with cg_update_xr_kernel's element
 //      mapping and CTA sum, and the same final reduction;
-//   C  p = r + beta p (elementwise).
+//   C  p = r + beta p (elementwise) -- or, in the two-barrier form, folded
+//      into the next iteration's phase A (see CoopFormPApEpi).
 // So the iterates are bit-identical to nm_cg_local's graph path.  Every CTA
 // computes the scalars itself (identically); CTA 0 publishes the final state.
 // Data written inside the kernel is read with ld.global.cg (L2), never through
-// the non-coherent read-only path.  Three grid barriers per iteration replace
-// the kernel boundaries; each wait is bounded (kWaitLimitNs): a CTA that gives
+// the non-coherent read-only path.  Three (two) grid barriers per iteration
+// replace the kernel boundaries; each wait is bounded (kWaitLimitNs): a CTA that gives
 // up sets the error word and the state to kCgDeviceError and leaves, and the
 // others give up at their next barrier.
 // ---------------------------------------------------------------------------
@@ -244,12 +245,40 @@ struct CoopPApEpi {
     __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
 };
 
-template <int TILE, int STAGES>
+// Row epilogue of the two-barrier form: the row's new direction
+// p'[row] = fma(beta, p[row], r[row]) (what the three-kernel path's p update
+// computes) goes to the other p buffer, then Ap and p'.Ap as in CoopPApEpi.
+struct CoopFormPApEpi {
+    static constexpr bool kBlockSums = false;
+    double* __restrict__ Ap;
+    const double* __restrict__ p;
+    const double* __restrict__ r;
+    double* __restrict__ pn;
+    double beta;
+    double dot;
+    __device__ __forceinline__ void operator()(int32_t row, double v) {
+        Ap[row] = v;
+        const double pr = fma(beta, __ldcg(p + row), __ldcg(r + row));
+        pn[row] = pr;
+        dot = fma(pr, v, dot);
+    }
+    __device__ __forceinline__ double take() { return 0.0; }
+    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+};
+
+// FORMED: the two-barrier form.  Phase C disappears: the next iteration's
+// SpMV multiplies by p' = fma(beta, p, r) formed from staged windows of p and
+// r (the same operation on the same operands in every CTA that reads a
+// column), and each row's owner writes p'[row] to the other p buffer for
+// phase B; the buffers alternate.  The first iteration forms p' = fma(0, p0,
+// r0) = r0 = p0.  Same iterates as the three-barrier form, one grid barrier
+// fewer per iteration, at the cost of a second set of staged windows.
+template <int TILE, int STAGES, bool FORMED>
 __global__ void __launch_bounds__(kCtaThreads)
-    cg_coop_kernel(CsrView<double> M, CgState* st, double* p, double* Ap, double* r,
+    cg_coop_kernel(CsrView<double> M, CgState* st, double* p, double* p2, double* Ap, double* r,
                    double* part_a, double* part_b, int grid_vec, int64_t n, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES>*>(smem_raw);
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES, FORMED>*>(smem_raw);
     __shared__ double bcast[2];
     __shared__ bool flag;
     const int t = threadIdx.x;
@@ -262,10 +291,24 @@ __global__ void __launch_bounds__(kCtaThreads)
     int32_t iter = __ldcg(&st->iter);
     M.coherent_x = 1;
     bool failed = false;
+    double beta_prev = 0.0;  // FORMED: beta of the previous iteration
     for (;;) {
-        // ---- A: Ap = A p, p.Ap ----
-        CoopPApEpi epi{Ap, p, 0.0};
-        const bool ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
+        // ---- A: Ap = A p, p.Ap (FORMED: p' = fma(beta_prev, p, r) formed on the fly) ----
+        double* pa_vec = p;  // the direction of this iteration
+        bool ok;
+        double dot;
+        if constexpr (FORMED) {
+            pa_vec = p2;
+            CoopFormPApEpi epi{Ap, p, r, p2, beta_prev, 0.0};
+            ok = spmv_pipeline<double, double, double, TILE, STAGES, true>(M, p, sm, epi, err,
+                                                                          AllBlocks(), r,
+                                                                          beta_prev);
+            dot = epi.dot;
+        } else {
+            CoopPApEpi epi{Ap, p, 0.0};
+            ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
+            dot = epi.dot;
+        }
         __syncthreads();
         if (t == 0) {  // the ring's barriers are initialised again by the next SpMV
 #pragma unroll
@@ -277,7 +320,7 @@ __global__ void __launch_bounds__(kCtaThreads)
             }
         }
         if (!ok) atomicExch(&st->status, kCgDeviceError);
-        const double pa = block_sum(epi.dot, sm.red);
+        const double pa = block_sum(dot, sm.red);
         if (t == 0) part_a[blockIdx.x] = pa;
         if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
         double s = 0.0;
@@ -303,7 +346,7 @@ __global__ void __launch_bounds__(kCtaThreads)
             double sv = 0.0;
             if (t < kThreads) {
                 for (int64_t i = int64_t(v) * kThreads + t; i < n; i += int64_t(grid_vec) * kThreads) {
-                    const double pi = __ldcg(p + i);
+                    const double pi = __ldcg(pa_vec + i);
                     x[i] = fma(alpha, pi, __ldcg(x + i));
                     const double ri = fma(-alpha, __ldcg(Ap + i), __ldcg(r + i));
                     r[i] = ri;
@@ -339,11 +382,19 @@ __global__ void __launch_bounds__(kCtaThreads)
             }
             return;
         }
-        // ---- C: p = r + beta p ----
-        for (int64_t i = int64_t(blockIdx.x) * blockDim.x + t; i < n;
-             i += int64_t(gridDim.x) * blockDim.x)
-            p[i] = fma(beta, __ldcg(p + i), __ldcg(r + i));
-        if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
+        if constexpr (FORMED) {
+            // the next SpMV forms p from this iteration's direction and r
+            double* const q = p;
+            p = p2;
+            p2 = q;
+            beta_prev = beta;
+        } else {
+            // ---- C: p = r + beta p ----
+            for (int64_t i = int64_t(blockIdx.x) * blockDim.x + t; i < n;
+                 i += int64_t(gridDim.x) * blockDim.x)
+                p[i] = fma(beta, __ldcg(p + i), __ldcg(r + i));
+            if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
+        }
     }
     if (failed && t == 0) {
         atomicExch(&st->status, kCgDeviceError);
@@ -414,17 +465,26 @@ int prepare_cg_spmv(int* occ) {
                           occ);
 }
 
-template <int TILE, int STAGES>
+template <int TILE, int STAGES, bool FORMED>
 int prepare_coop(int* occ) {
-    return prepare_kernel(reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES>),
-                          kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(),
-                          occ);
+    return prepare_kernel(reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES, FORMED>),
+                          kCtaThreads,
+                          spmv_smem_bytes<double, double, double, TILE, STAGES, FORMED>(), occ);
 }
 
-template <int TILE>
+template <int TILE, bool FORMED>
 int prepare_coop_s(int stages, int* occ) {
-    if (stages == 4) return prepare_coop<TILE, 4>(occ);
-    return stages == 3 ? prepare_coop<TILE, 3>(occ) : prepare_coop<TILE, 2>(occ);
+    if (stages == 4) return prepare_coop<TILE, 4, FORMED>(occ);
+    return stages == 3 ? prepare_coop<TILE, 3, FORMED>(occ) : prepare_coop<TILE, 2, FORMED>(occ);
+}
+
+template <bool FORMED>
+int prepare_coop_t(int tile, int stages, int* occ) {
+    switch (tile) {
+        case 1024: return prepare_coop_s<1024, FORMED>(stages, occ);
+        case 4096: return prepare_coop_s<4096, FORMED>(stages, occ);
+        default: return prepare_coop_s<2048, FORMED>(stages, occ);
+    }
 }
 
 template <int TILE>
@@ -460,34 +520,36 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     ws->grid_spmv = spmv_grid(A, occ);
     ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
     {
-        // r, p, Ap, the CTA partial sums and the state in one allocation
+        // r, p, Ap, p2, the CTA partial sums and the state in one allocation
         // (each part 256-byte aligned)
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         const size_t vb = up(sizeof(double) * size_t(n));
         const size_t pb = up(sizeof(double) * size_t(ws->partials_cap));
-        NM_CUDA_TRY(cudaMalloc(&ws->dmem, 3 * vb + pb + up(sizeof(CgState))));
+        NM_CUDA_TRY(cudaMalloc(&ws->dmem, 4 * vb + pb + up(sizeof(CgState))));
         auto* base = static_cast<unsigned char*>(ws->dmem);
         ws->r = reinterpret_cast<double*>(base);
         ws->p = reinterpret_cast<double*>(base + vb);
         ws->Ap = reinterpret_cast<double*>(base + 2 * vb);
-        ws->partials = reinterpret_cast<double*>(base + 3 * vb);
-        ws->st = reinterpret_cast<CgState*>(base + 3 * vb + pb);  // written by every solve
+        ws->p2 = reinterpret_cast<double*>(base + 3 * vb);
+        ws->partials = reinterpret_cast<double*>(base + 4 * vb);
+        ws->st = reinterpret_cast<CgState*>(base + 4 * vb + pb);  // written by every solve
     }
     {
         // The persistent solve runs on the same grid, every CTA resident.
-        int dev = 0, coop_ok = 0, occ_c = 0;
+        int dev = 0, coop_ok = 0, occ_c = 0, occ_f = 0;
         NM_CUDA_TRY(cudaGetDevice(&dev));
         NM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
-        switch (A->tune.tile) {
-            case 1024: st = prepare_coop_s<1024>(A->tune.stages, &occ_c); break;
-            case 4096: st = prepare_coop_s<4096>(A->tune.stages, &occ_c); break;
-            default: st = prepare_coop_s<2048>(A->tune.stages, &occ_c); break;
-        }
+        st = prepare_coop_t<false>(A->tune.tile, A->tune.stages, &occ_c);
+        if (st != NM_OK) return st;
+        st = prepare_coop_t<true>(A->tune.tile, A->tune.stages, &occ_f);
         if (st != NM_OK) return st;
         // Large systems keep the graph path: their update phases need more CTAs
-        // than the SpMV grid has.
+        // than the SpMV grid has.  The two-barrier form stages twice the
+        // windows, so fewer of its CTAs fit an SM; where the grid does not fit
+        // it, the three-barrier form runs.
         ws->coop = coop_ok && int64_t(occ_c) * sm_count() >= ws->grid_spmv &&
                    n <= kCoopMaxRows;
+        ws->coop_formed = ws->coop && int64_t(occ_f) * sm_count() >= ws->grid_spmv;
     }
     ws->err = device_error_word();
     if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
@@ -548,35 +610,41 @@ int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* ou
     return NM_OK;
 }
 
-template <int TILE, int STAGES>
+template <int TILE, int STAGES, bool FORMED>
 int launch_coop_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
     CsrView<double> M = A->view<double>();
-    M.stage_x = 1;  // p is a workspace vector (256-byte aligned)
+    M.stage_x = 1;  // p, p2 and r are workspace vectors (256-byte aligned)
     double* part_a = ws->partials;
     double* part_b = ws->partials + ws->grid_spmv;
     int grid_vec = ws->grid_vec;
     int64_t n = ws->n;
-    void* args[] = {&M, &ws->st, &ws->p, &ws->Ap, &ws->r, &part_a, &part_b, &grid_vec, &n,
-                    &ws->err};
+    void* args[] = {&M,     &ws->st, &ws->p,    &ws->p2, &ws->Ap, &ws->r,
+                    &part_a, &part_b, &grid_vec, &n,      &ws->err};
     NM_CUDA_TRY(cudaLaunchCooperativeKernel(
-        reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES>), dim3(ws->grid_spmv),
-        dim3(kCtaThreads), args, spmv_smem_bytes<double, double, double, TILE, STAGES>(), s));
+        reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES, FORMED>),
+        dim3(ws->grid_spmv), dim3(kCtaThreads), args,
+        spmv_smem_bytes<double, double, double, TILE, STAGES, FORMED>(), s));
     return NM_OK;
 }
 
-template <int TILE>
+template <int TILE, bool FORMED>
 int launch_coop_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
-    if (A->tune.stages == 4) return launch_coop_t<TILE, 4>(A, ws, s);
-    if (A->tune.stages == 3) return launch_coop_t<TILE, 3>(A, ws, s);
-    return launch_coop_t<TILE, 2>(A, ws, s);
+    if (A->tune.stages == 4) return launch_coop_t<TILE, 4, FORMED>(A, ws, s);
+    if (A->tune.stages == 3) return launch_coop_t<TILE, 3, FORMED>(A, ws, s);
+    return launch_coop_t<TILE, 2, FORMED>(A, ws, s);
+}
+
+template <bool FORMED>
+int launch_coop_f(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+    switch (A->tune.tile) {
+        case 1024: return launch_coop_s<1024, FORMED>(A, ws, s);
+        case 4096: return launch_coop_s<4096, FORMED>(A, ws, s);
+        default: return launch_coop_s<2048, FORMED>(A, ws, s);
+    }
 }
 
 int launch_coop(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
-    switch (A->tune.tile) {
-        case 1024: return launch_coop_s<1024>(A, ws, s);
-        case 4096: return launch_coop_s<4096>(A, ws, s);
-        default: return launch_coop_s<2048>(A, ws, s);
-    }
+    return ws->coop_formed ? launch_coop_f<true>(A, ws, s) : launch_coop_f<false>(A, ws, s);
 }
 
 }  // namespace

@@ -33,13 +33,15 @@ constexpr int kCgDeviceError = 2;
 struct CgWorkspace {
     int64_t n = 0;
     bool coop = false;  // the persistent cooperative solve fits this matrix's SpMV grid
+    bool coop_formed = false;  // ... in its two-barrier form (p formed inside the SpMV)
     double* r = nullptr;
     double* p = nullptr;
+    double* p2 = nullptr;  // second p buffer of the two-barrier persistent solve
     double* Ap = nullptr;
     double* partials = nullptr;
     int partials_cap = 0;
     CgState* st = nullptr;
-    void* dmem = nullptr;       // one device allocation holding r, p, Ap, partials, st
+    void* dmem = nullptr;       // one device allocation holding r, p, p2, Ap, partials, st
     CgState* h_in = nullptr;    // pinned staging of the inputs (a slot of a shared slab)
     CgState* h_out = nullptr;   // pinned landing of the outputs (idem)
     int grid_spmv = 0, grid_vec = 0;

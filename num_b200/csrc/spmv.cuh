@@ -44,6 +44,8 @@
 // CTA exits.
 #pragma once
 
+#include <type_traits>
+
 #include "csr.cuh"
 
 namespace nm {
@@ -98,9 +100,16 @@ struct alignas(16) SpmvStage {
     X xw[xwin_capacity(TILE)];  // the block's x windows, back to back
 };
 
-template <typename V, typename X, typename A, int TILE, int STAGES>
+// With XR the stage also holds the same windows of a second vector xr: the
+// pipeline then multiplies by x' = fma(beta, x, xr), formed as it is read.
+template <typename V, typename X, int TILE>
+struct alignas(16) SpmvStageXR : SpmvStage<V, X, TILE> {
+    X xrw[xwin_capacity(TILE)];
+};
+
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR = false>
 struct SpmvSmem {
-    SpmvStage<V, X, TILE> st[STAGES];
+    std::conditional_t<XR, SpmvStageXR<V, X, TILE>, SpmvStage<V, X, TILE>> st[STAGES];
     uint64_t full[STAGES];
     uint64_t empty[STAGES];
     BlockDesc meta[STAGES];  // descriptor of the block in each stage
@@ -130,10 +139,10 @@ struct AllBlocks {
 // row_ptr slice and, when M.stage_x, its x windows).  A block the gate
 // rejected (d.aux.z = 1, decided when the descriptor was loaded) is not
 // staged; it reaches the consumers marked skipped.
-template <typename V, typename X, typename A, int TILE, int STAGES>
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR = false>
 __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restrict__ x,
-                                           BlockDesc d, SpmvSmem<V, X, A, TILE, STAGES>& sm,
-                                           int s) {
+                                           BlockDesc d, SpmvSmem<V, X, A, TILE, STAGES, XR>& sm,
+                                           int s, const X* __restrict__ xr = nullptr) {
     const int32_t r0 = d.rz.x, r1 = d.rz.y, z0 = d.rz.z, z1 = d.rz.w;
     const bool skip = d.aux.z != 0;
     const bool long_row = z1 - z0 > TILE;
@@ -149,9 +158,9 @@ __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restr
     const uint32_t ncol = static_cast<uint32_t>(a1 - a0);
     const uint32_t nrp = static_cast<uint32_t>(ra1 - ra0);
     const uint32_t nxw = stage_x ? static_cast<uint32_t>(d.xl.x + d.xl.y + d.xl.z + d.xl.w) : 0u;
-    const uint32_t bytes =
-        ncol * uint32_t(sizeof(int32_t) + sizeof(V)) + nrp * 4u + nxw * uint32_t(sizeof(X));
-    SpmvStage<V, X, TILE>& st = sm.st[s];
+    const uint32_t bytes = ncol * uint32_t(sizeof(int32_t) + sizeof(V)) + nrp * 4u +
+                           nxw * uint32_t(sizeof(X)) * (XR ? 2u : 1u);
+    auto& st = sm.st[s];
     mbar_arrive_expect_tx(&sm.full[s], bytes);
     if (ncol) {
         bulk_g2s(st.col, M.col_idx + a0, ncol * 4u, &sm.full[s]);
@@ -164,9 +173,13 @@ __device__ __forceinline__ void spmv_issue(const CsrView<V>& M, const X* __restr
         int32_t off = 0;
 #pragma unroll
         for (int k = 0; k < kXSeg; ++k) {
-            if (wl[k] > 0)
+            if (wl[k] > 0) {
                 bulk_g2s(st.xw + off, x + ws[k], uint32_t(wl[k]) * uint32_t(sizeof(X)),
                          &sm.full[s]);
+                if constexpr (XR)
+                    bulk_g2s(st.xrw + off, xr + ws[k], uint32_t(wl[k]) * uint32_t(sizeof(X)),
+                             &sm.full[s]);
+            }
             off += wl[k];
         }
     }
@@ -179,11 +192,24 @@ __device__ __forceinline__ X load_x(const CsrView<V>& M, const X* p) {
     return M.coherent_x ? __ldcg(p) : __ldg(p);
 }
 
+// Entry c of the multiplied vector: x[c], or with XR fma(beta, x[c], xr[c]).
+template <bool XR, typename V, typename X>
+__device__ __forceinline__ X load_xop(const CsrView<V>& M, const X* x, const X* xr, X beta,
+                                      int32_t c) {
+    if constexpr (XR) {
+        static_assert(std::is_same_v<X, double>, "a formed x' is FP64 only");
+        return fma(beta, load_x(M, x + c), load_x(M, xr + c));
+    } else {
+        return load_x(M, x + c);
+    }
+}
+
 // One long row (nnz > TILE) straight from global memory, all consumers.
-template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR, class Epi>
 __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int32_t r0,
                                               int32_t z0, int32_t z1, const X* __restrict__ x,
-                                              SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
+                                              SpmvSmem<V, X, A, TILE, STAGES, XR>& sm, Epi& epi,
+                                              const X* __restrict__ xr, X beta) {
     const int t = threadIdx.x;
     A s = A(0);
     for (int32_t j = (z0 & ~3) + 4 * t; ok && j < z1; j += 4 * kConsumers) {
@@ -194,7 +220,8 @@ __device__ __forceinline__ void spmv_long_row(const CsrView<V>& M, bool ok, int3
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int32_t jj = j + q;
-            if (jj >= z0 && jj < z1) s += v[q] * static_cast<A>(load_x(M, x + cc[q]));
+            if (jj >= z0 && jj < z1)
+                s += v[q] * static_cast<A>(load_xop<XR>(M, x, xr, beta, cc[q]));
         }
     }
     s = consumer_sum(s, sm.red);
@@ -219,13 +246,14 @@ __device__ __forceinline__ A* prod_slots(SpmvStage<V, X, TILE>& st) {
     }
 }
 
-template <typename V, typename X, typename A, int TILE, int STAGES, class Epi>
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR, class Epi>
 __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, const BlockDesc& d,
                                           const X* __restrict__ x,
-                                          SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi) {
+                                          SpmvSmem<V, X, A, TILE, STAGES, XR>& sm, Epi& epi,
+                                          const X* __restrict__ xr, X beta) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
-    SpmvStage<V, X, TILE>& st = sm.st[s];
+    auto& st = sm.st[s];
     const int32_t r0 = d.rz.x, z0 = d.rz.z;
     const int nr = d.rz.y - r0;
     const int32_t a0 = z0 & ~7;
@@ -235,7 +263,10 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
                   dl3 = d.xl.x + d.xl.y + d.xl.z - d.xs.w;
     auto xval = [&](int32_t c) -> A {
         const int32_t dl = c >= d.xs.w ? dl3 : (c >= d.xs.z ? dl2 : (c >= d.xs.y ? dl1 : dl0));
-        return static_cast<A>(st.xw[c + dl]);
+        if constexpr (XR)
+            return static_cast<A>(fma(beta, st.xw[c + dl], st.xrw[c + dl]));
+        else
+            return static_cast<A>(st.xw[c + dl]);
     };
 
     // A block without staged x windows (scattered columns) gathers first:
@@ -266,7 +297,12 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
                 // through L2 (ld.global.cg): scattered columns rarely hit L1,
                 // and skipping it raises the gather rate (power-law rows:
                 // 299 -> 248 us per SpMV)
-                if (j0 + g * kConsumers < j1) xv[g] = static_cast<A>(__ldcg(x + c[g]));
+                if (j0 + g * kConsumers < j1) {
+                    if constexpr (XR)
+                        xv[g] = static_cast<A>(fma(beta, __ldcg(x + c[g]), __ldcg(xr + c[g])));
+                    else
+                        xv[g] = static_cast<A>(__ldcg(x + c[g]));
+                }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int32_t j = j0 + g * kConsumers;
@@ -347,11 +383,15 @@ __device__ __forceinline__ void spmv_rows(const CsrView<V>& M, int s, bool ok, c
 // threads.  Returns false on the threads of a CTA where a bounded wait gave
 // up (the error word is set; partial results must not be used).  On return
 // no TMA copy into this CTA's shared memory is pending.
-template <typename V, typename X, typename A, int TILE, int STAGES, class Epi,
+// With XR the vector multiplied is x' = fma(beta, x, xr), formed from staged
+// windows of both (or gathered pairs) as it is read.
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR = false, class Epi,
           class Gate = AllBlocks>
 __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict__ x,
-                                              SpmvSmem<V, X, A, TILE, STAGES>& sm, Epi& epi,
-                                              unsigned int* err, const Gate& gate = Gate()) {
+                                              SpmvSmem<V, X, A, TILE, STAGES, XR>& sm, Epi& epi,
+                                              unsigned int* err, const Gate& gate = Gate(),
+                                              const X* __restrict__ xr = nullptr,
+                                              X beta = X(0)) {
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
     if (M.nblk_dev) M.nblk = __ldg(M.nblk_dev);
@@ -403,7 +443,7 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
                 finish(s);
             }
             sm.bid[s] = b;
-            spmv_issue<V, X, A, TILE, STAGES>(M, x, d, sm, s);
+            spmv_issue<V, X, A, TILE, STAGES, XR>(M, x, d, sm, s, xr);
             full_par ^= 1u << s;
             used |= 1u << s;
             s = (s + 1 == STAGES) ? 0 : s + 1;
@@ -449,9 +489,10 @@ __device__ __forceinline__ bool spmv_pipeline(CsrView<V> M, const X* __restrict_
         // consumers that saw the stage and consumers that gave up stay in step.
         const bool active = ok && d.aux.z == 0;
         if (d.rz.w - d.rz.z > TILE)
-            spmv_long_row<V, X, A, TILE, STAGES>(M, active, d.rz.x, d.rz.z, d.rz.w, x, sm, epi);
+            spmv_long_row<V, X, A, TILE, STAGES, XR>(M, active, d.rz.x, d.rz.z, d.rz.w, x, sm,
+                                                     epi, xr, beta);
         else
-            spmv_rows<V, X, A, TILE, STAGES>(M, s, active, d, x, sm, epi);
+            spmv_rows<V, X, A, TILE, STAGES, XR>(M, s, active, d, x, sm, epi, xr, beta);
         if constexpr (Epi::kBlockSums) {
             const double v = warp_sum(epi.take());
             if (lane == 0) sm.blk_red[s][warp] = v;  // published by the arrival below
@@ -474,9 +515,9 @@ struct StoreEpi {
 };
 
 // Dynamic shared memory of the pipelined kernels.
-template <typename V, typename X, typename A, int TILE, int STAGES>
+template <typename V, typename X, typename A, int TILE, int STAGES, bool XR = false>
 constexpr size_t spmv_smem_bytes() {
-    return sizeof(SpmvSmem<V, X, A, TILE, STAGES>);
+    return sizeof(SpmvSmem<V, X, A, TILE, STAGES, XR>);
 }
 
 }  // namespace nm

@@ -246,13 +246,44 @@ def test_vector_ops_bit_exact(nmlib, kspmv, oracle):
     assert nmlib.nm_dot(0, None, None, C.byref(zero), s) == 0 and zero.value == 0.0
 
 
-@pytest.mark.parametrize("case", ["lap2d_256", "lap3d_64", "varcoef_48", "banded"])
+def _arrow_spd(n, rng):
+    """Row 0 (and column 0) dense, the rest diagonal: row 0 is one block with
+    more nonzeros than a tile (the long-row path)."""
+    u = 0.01 * rng.uniform(-1, 1, n)
+    d = 1.0 + rng.uniform(0, 1, n)
+    d[0] = 1.0 + np.abs(u[1:]).sum()
+    rp = np.empty(n + 1, np.int32)
+    rp[0], rp[1] = 0, n
+    rp[2:] = n + 2 * np.arange(1, n, dtype=np.int64)
+    ci = np.empty(n + 2 * (n - 1), np.int32)
+    v = np.empty(ci.shape[0])
+    ci[:n] = np.arange(n)
+    v[:n] = np.concatenate([[d[0]], u[1:]])
+    ci[n::2], ci[n + 1::2] = 0, np.arange(1, n)
+    v[n::2], v[n + 1::2] = u[1:], d[1:]
+    return gen.Csr(rp, ci, v, n, n)
+
+
+# The persistent solve runs in its two-barrier form (direction formed inside
+# the SpMV) while the SpMV grid fits it -- the 256^2 and 40^3 Laplacians, the
+# 30,000-row banded system (scattered off-band columns: the gather path) and
+# the arrow matrix (a long row) -- and in its three-barrier form for the
+# 64^3 Laplacian and the 48^3 variable-coefficient system (grids of 444 and
+# 432 CTAs); the 300,000-row banded system takes the graph path both ways.
+@pytest.mark.parametrize("case", ["lap2d_256", "lap3d_40", "banded_30k", "arrow_20k",
+                                  "lap3d_64", "varcoef_48", "banded"])
 def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
     # nm_cg_local runs the whole solve in one cooperative launch by default;
     # the three-kernel CUDA-graph path must give the same bits.
     rng = np.random.default_rng(21)
     if case == "lap2d_256":
         A = gen.laplacian_2d(256)
+    elif case == "lap3d_40":
+        A = gen.laplacian_3d(40)
+    elif case == "banded_30k":
+        A = gen.banded_spd(30_000, 5, rng)
+    elif case == "arrow_20k":
+        A = _arrow_spd(20_000, rng)
     elif case == "lap3d_64":
         A = gen.laplacian_3d(64)
     elif case == "varcoef_48":
