@@ -297,7 +297,8 @@ def run_spmv(args, rank, world, local_rank):
     else:
         # the project's autotuner picks the partition and launch shape
         at = kspmv.autotune(M, budget_ms=200, cache=False)
-        tuned = {k: at[k] for k in ("tile", "max_rows", "short_max", "grid_mult", "stages")}
+        tuned = {k: at[k] for k in ("tile", "max_rows", "short_max", "grid_mult", "stages",
+                                    "kernel")}
         tuned["chosen_by"] = f"autotune ({len(at['trials'])} candidates timed)"
     dt = torch.float64 if precision == "fp64" else torch.float32
     xd = torch.tensor(x, dtype=dt, device=dev)
@@ -385,7 +386,9 @@ def run_spmv(args, rank, world, local_rank):
             "frac": round(achieved / peak, 4), "peak_source": peak_src,
             "frac_of_8TBs_spec": round(achieved / 8000.0, 4),
             "traffic": traffic_for(args.workload),
-            "kernel": "nm::spmv_kernel (row-block CSR SpMV)",
+            "kernel": ("nm::spmv_gather_kernel (warp per 32 rows, x gathered through L2)"
+                       if kspmv.spmv_kernel(M) == "gather"
+                       else "nm::spmv_kernel (row-block CSR SpMV)"),
             "kernel_avg_us": round(kern_avg_ms * 1e3, 3),
         },
         "e2e": {

@@ -52,7 +52,16 @@ typedef struct {
     int32_t short_max;  /* rows with <= short_max nonzeros: one thread; else a warp */
     int32_t grid_mult;  /* CTAs launched per SM by the persistent SpMV grid (0: auto) */
     int32_t stages;     /* TMA pipeline depth of the SpMV kernels: 2, 3 or 4          */
+    int32_t kernel;     /* plain SpMV kernel: NM_KERNEL_AUTO / _BLOCKS / _GATHER      */
 } nm_tuning;
+
+/* nm_tuning.kernel.  BLOCKS: the row-block TMA pipeline.  GATHER: one warp per
+ * 32 rows streaming the nonzeros and gathering x through L2, every row summed
+ * serially in CSR order (for scattered columns).  AUTO: GATHER when at least
+ * 3/4 of the nonzeros lie in row blocks without x windows and no row has more
+ * than 4096 nonzeros, else BLOCKS.  CG and the batched engine always use the
+ * row-block pipeline. */
+enum nm_kernel { NM_KERNEL_AUTO = 1, NM_KERNEL_BLOCKS = 2, NM_KERNEL_GATHER = 3 };
 
 typedef struct nm_csr nm_csr;    /* device CSR matrix (CrsMatrixHandle)   */
 typedef struct nm_dist nm_dist;  /* one rank's slice (DistCrsHandle)      */
@@ -127,11 +136,15 @@ int nm_csr_info(const nm_csr* A, int32_t* nrows, int32_t* ncols, int32_t* nnz,
 
 /* Replaces pick_rows_per_team (src/spmv_kernel.hpp:102-109): sets the
  * row-block partition parameters and rebuilds the partition.  tile,
- * max_rows, short_max and stages <= 0 (grid_mult < 0) keep their current
- * values; grid_mult 0 selects the automatic grid.  Defaults: 2048, 256, 32,
- * 0, 2. */
+ * max_rows, short_max, stages and kernel <= 0 (grid_mult < 0) keep their
+ * current values; grid_mult 0 selects the automatic grid.  Defaults: 2048,
+ * 256, 32, 0, 2, NM_KERNEL_AUTO. */
 int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t);
 int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t);
+
+/* The plain-SpMV kernel nm_spmv runs on A under its tuning (AUTO resolved):
+ * NM_KERNEL_BLOCKS or NM_KERNEL_GATHER. */
+int nm_csr_spmv_kernel(const nm_csr* A, int32_t* kernel);
 
 /* One timed candidate of nm_csr_autotune. */
 typedef struct {
@@ -142,7 +155,8 @@ typedef struct {
 /* SpMV autotuner (no reference counterpart; the reference's partition is
  * fixed).  Times y = A*x on `stream` under every candidate tile (1024, 2048,
  * 4096), short_max (32, 64), stages (2, 3, 4; those whose shared memory fits)
- * and grid_mult (0, 1, 2), spending about budget_ms of device time (<= 0:
+ * and grid_mult (0, 1, 2) of the row-block kernel, and the warp-gather
+ * kernel, spending about budget_ms of device time (<= 0:
  * 200 ms), installs the fastest on A and returns it in *best.  x is read; y
  * is overwritten.  trials[0..min(cap, *ntrials)) receive every timing (trials
  * may be NULL when cap is 0).  Synchronises `stream`. */

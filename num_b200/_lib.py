@@ -33,7 +33,7 @@ class SolverOpts(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tile", C.c_int32), ("max_rows", C.c_int32), ("short_max", C.c_int32),
-                ("grid_mult", C.c_int32), ("stages", C.c_int32)]
+                ("grid_mult", C.c_int32), ("stages", C.c_int32), ("kernel", C.c_int32)]
 
 
 class SolverCounters(C.Structure):
@@ -61,6 +61,7 @@ _SIGNATURES = {
     "nm_csr_create_batched": ([i32, vp, vp, vp, vp, vp, C.c_int, C.POINTER(vp)], C.c_int),
     "nm_csr_destroy": ([vp], C.c_int),
     "nm_csr_laplacian": ([i32, i32, C.c_int, C.POINTER(vp)], C.c_int),
+    "nm_csr_spmv_kernel": ([vp, P_i32], C.c_int),
     "nm_csr_export": ([vp, vp, vp, vp], C.c_int),
     "nm_csr_info": ([vp, P_i32, P_i32, P_i32, P_i32, P_i32], C.c_int),
     "nm_csr_set_tuning": ([vp, C.POINTER(Tuning)], C.c_int),

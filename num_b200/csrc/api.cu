@@ -148,7 +148,7 @@ extern "C" int nm_row_blocks_host(const int32_t* row_ptr, int32_t nrows, const n
     nm::clear_error();
     if (!row_ptr || !blk || !nblk || nrows < 0)
         return fail(NM_ERR_INVALID, "nm_row_blocks_host: bad argument");
-    nm_tuning tt = t ? *t : nm_tuning{0, 0, 0, 0, 0};
+    nm_tuning tt = t ? *t : nm_tuning{0, 0, 0, 0, 0, 0};
     if (tt.tile <= 0) tt.tile = nm::kDefaultTile;
     if (tt.max_rows <= 0) tt.max_rows = nm::kDefaultMaxRows;
     if (tt.short_max <= 0) tt.short_max = nm::kDefaultShortMax;

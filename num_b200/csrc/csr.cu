@@ -116,6 +116,10 @@ int normalise_tuning(nm_tuning& t) {
     if (t.short_max <= 0) t.short_max = kDefaultShortMax;
     if (t.grid_mult < 0) t.grid_mult = 0;
     if (t.stages <= 0) t.stages = kDefaultStages;
+    if (t.kernel <= 0) t.kernel = NM_KERNEL_AUTO;
+    if (t.kernel > NM_KERNEL_GATHER)
+        return fail(NM_ERR_INVALID, "tuning: kernel must be 1 (auto), 2 (blocks) or 3 (gather) "
+                    "(got %d)", t.kernel);
     if (t.stages < 2 || t.stages > 4)
         return fail(NM_ERR_INVALID, "tuning: stages must be 2, 3 or 4 (got %d)", t.stages);
     if (t.tile != 1024 && t.tile != 2048 && t.tile != 4096)
@@ -205,6 +209,19 @@ int rebuild_blocks(nm_csr* A) {
             th.emplace_back(fill, int32_t(int64_t(nb) * i / nthr), int32_t(int64_t(nb) * (i + 1) / nthr));
         for (auto& t : th) t.join();
     }
+    {
+        // Scattered columns (at least 3/4 of the nonzeros in blocks without x
+        // windows) and no long row: the plain SpMV gathers warp by warp.
+        int64_t gathered = 0;
+        for (int32_t b = 0; b < nb; ++b)
+            if (desc[b].xs.x < 0) gathered += desc[b].rz.w - desc[b].rz.z;
+        int32_t max_row = 0;
+        for (int32_t r = 0; r < A->nrows; ++r) max_row = std::max(max_row, rp[r + 1] - rp[r]);
+        const bool scattered = A->nnz > 0 && 4 * gathered >= 3 * int64_t(A->nnz) &&
+                               max_row <= kWarpGatherMaxRow;
+        A->warp_gather = A->tune.kernel == NM_KERNEL_GATHER ||
+                         (A->tune.kernel == NM_KERNEL_AUTO && scattered);
+    }
     if (A->d_blk) {
         cudaFree(A->d_blk);
         A->d_blk = nullptr;
@@ -285,7 +302,7 @@ extern "C" int nm_csr_create(const int32_t* row_ptr, const int32_t* col_idx, con
     A->ncols = ncols;
     A->nnz = row_ptr[nrows];
     A->dtype = dtype;
-    A->tune = nm_tuning{0, 0, 0, 0, 0};
+    A->tune = nm_tuning{0, 0, 0, 0, 0, 0};
     nm::normalise_tuning(A->tune);
     return nm::finish_create(A, row_ptr, col_idx, values, out);
 }
@@ -341,7 +358,7 @@ extern "C" int nm_csr_create_batched(int32_t count, const int32_t* nrows, const 
     A->ncols = static_cast<int32_t>(tot_cols);
     A->nnz = static_cast<int32_t>(tot_nnz);
     A->dtype = dtype;
-    A->tune = nm_tuning{0, 0, 0, 0, 0};
+    A->tune = nm_tuning{0, 0, 0, 0, 0, 0};
     nm::normalise_tuning(A->tune);
     A->batch_row_off = row_off;
     A->batch_col_off = col_off;
@@ -372,7 +389,7 @@ extern "C" int nm_csr_laplacian(int32_t dim, int32_t L, int dtype, nm_csr** out)
     A->nrows = A->ncols = static_cast<int32_t>(n);
     A->nnz = static_cast<int32_t>(nnz);
     A->dtype = dtype;
-    A->tune = nm_tuning{0, 0, 0, 0, 0};
+    A->tune = nm_tuning{0, 0, 0, 0, 0, 0};
     nm::normalise_tuning(A->tune);
     auto build = [&]() -> int {
         // Same allocation and padding as an uploaded matrix.
@@ -448,6 +465,7 @@ extern "C" int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t) {
     if (nt.short_max <= 0) nt.short_max = A->tune.short_max;
     if (nt.grid_mult < 0) nt.grid_mult = A->tune.grid_mult;
     if (nt.stages <= 0) nt.stages = A->tune.stages;
+    if (nt.kernel <= 0) nt.kernel = A->tune.kernel;
     int st = nm::normalise_tuning(nt);
     if (st != NM_OK) return st;
     {
@@ -457,6 +475,13 @@ extern "C" int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t) {
     }
     A->tune = nt;
     return nm::rebuild_blocks(A);
+}
+
+extern "C" int nm_csr_spmv_kernel(const nm_csr* A, int32_t* kernel) {
+    nm::clear_error();
+    if (!A || !kernel) return fail(NM_ERR_INVALID, "nm_csr_spmv_kernel: NULL argument");
+    *kernel = A->warp_gather ? NM_KERNEL_GATHER : NM_KERNEL_BLOCKS;
+    return NM_OK;
 }
 
 extern "C" int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t) {

@@ -90,6 +90,10 @@ struct nm_csr {
     nm::BlockDesc* d_desc = nullptr;
     int32_t nblk = 0;
     nm_tuning tune{};
+    // Plain SpMV by the warp-gather kernel (spmv.cu): set by rebuild_blocks
+    // from tune.kernel (AUTO: most nonzeros in blocks without x windows and no
+    // row longer than kWarpGatherMaxRow).
+    bool warp_gather = false;
     std::vector<int32_t> h_row_ptr;  // kept to rebuild the partition on retuning
     std::vector<int32_t> h_col_idx;  // kept to rebuild the x windows on retuning
     // Many-matrix handles: per-matrix row / column offsets (count + 1 each).
@@ -114,8 +118,11 @@ int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t stream);
 // Dynamic shared memory of the SpMV kernel for (dtype, tile, stages); 0 if
 // the combination does not exist.
 size_t spmv_smem_for(int dtype, int tile, int stages);
-// Rebuilds the row-block partition and descriptors of A under A->tune.
+// Rebuilds the row-block partition and descriptors of A under A->tune (and
+// the choice of plain-SpMV kernel).
 int rebuild_blocks(nm_csr* A);
+// Longest row the warp-gather kernel takes (each row is summed by one lane).
+constexpr int32_t kWarpGatherMaxRow = 4096;
 // Drops A's cached CG workspace (its graphs hold the current descriptors).
 void reset_cg(nm_csr* A);
 // Nonzeros of the Laplacian on an L^dim grid (dim 2: 5-point, dim 3: 7-point).

@@ -6,6 +6,7 @@
 //   short_max 32, 64             rows up to this length are thread-per-row
 //   stages    2, 3, 4            TMA ring depth (skipped when it does not fit)
 //   grid_mult 0 (all resident CTAs), 1, 2 CTAs per SM
+//   and, once, the warp-gather kernel (which ignores the four above)
 // max_rows stays at its default (one consumer thread per row of a block).
 // tile and short_max change the descriptors (a host rebuild per pair);
 // stages and grid_mult only change the launch.  short_max never goes below
@@ -70,7 +71,7 @@ extern "C" int nm_csr_autotune(nm_csr* A, const void* x, void* y, void* stream,
     float t0 = 0.f;
     int st = time_spmv(A, x, y, s, 2, 3, ev.a, ev.b, &t0);
     if (st != NM_OK) return st;
-    constexpr int kCandidates = 3 * 2 * 3 * 3;
+    constexpr int kCandidates = 3 * 2 * 3 * 3 + 1;
     const double budget_us = (budget_ms > 0 ? budget_ms : 200.0) * 1000.0;
     const int reps = int(std::max(3.0, std::min(200.0, budget_us / kCandidates / std::max(1.f, t0))));
     const int32_t tiles[] = {1024, 2048, 4096};
@@ -89,6 +90,7 @@ extern "C" int nm_csr_autotune(nm_csr* A, const void* x, void* y, void* stream,
             t.max_rows = kDefaultMaxRows;
             t.stages = 2;
             t.grid_mult = 0;
+            t.kernel = NM_KERNEL_BLOCKS;
             A->tune = t;
             st = rebuild_blocks(A);
             if (st != NM_OK) break;
@@ -112,6 +114,23 @@ extern "C" int nm_csr_autotune(nm_csr* A, const void* x, void* y, void* stream,
                 }
             if (st != NM_OK) break;
         }
+    if (st == NM_OK) {
+        nm_tuning t = start;
+        t.kernel = NM_KERNEL_GATHER;
+        A->tune = t;
+        st = rebuild_blocks(A);
+        float us = 0.f;
+        if (st == NM_OK) st = time_spmv(A, x, y, s, 1, reps, ev.a, ev.b, &us);
+        if (st == NM_OK) {
+            if (n < cap) trials[n] = nm_tune_trial{A->tune, us};
+            ++n;
+            if (!have || us < win_us) {
+                win = A->tune;
+                win_us = us;
+                have = true;
+            }
+        }
+    }
     if (ntrials) *ntrials = n;
     // Install the winner (or put the starting tuning back on failure).
     const nm_tuning fin = (st == NM_OK && have) ? win : start;

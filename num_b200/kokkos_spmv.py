@@ -36,9 +36,12 @@ __all__ = [
     "init", "finalize", "rank", "size", "barrier", "CrsMatrix", "DistCrsMatrix", "upload_csr",
     "upload_csr_batched", "distribute_csr", "spmv", "batch_spmv", "dist_spmv", "cg_solve",
     "cg_solve_local", "tune", "tuning", "autotune", "row_blocks", "laplacian", "download_csr",
+    "spmv_kernel",
 ]
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
+# nm_tuning.kernel: the plain SpMV kernel (auto, the row-block pipeline, the warp gather)
+_KERNELS = {"auto": 1, "blocks": 2, "gather": 3}
 
 
 def _dist():
@@ -385,19 +388,37 @@ def cg_solve(A_dist: DistCrsMatrix, b, x, tol: float = 1e-10, max_iter: int = 10
 # ---- additions -----------------------------------------------------------------
 
 def tuning(A: CrsMatrix) -> dict:
-    """The row-block partition parameters of A."""
+    """The row-block partition parameters of A and its plain-SpMV kernel."""
     out = _lib.Tuning()
     _lib.check(_lib.load().nm_csr_get_tuning(A._h, C.byref(out)))
+    names = {v: k for k, v in _KERNELS.items()}
     return {"tile": out.tile, "max_rows": out.max_rows, "short_max": out.short_max,
-            "grid_mult": out.grid_mult, "stages": out.stages}
+            "grid_mult": out.grid_mult, "stages": out.stages, "kernel": names[out.kernel]}
+
+
+def spmv_kernel(A: CrsMatrix) -> str:
+    """The kernel spmv runs on A: "blocks" (row-block pipeline) or "gather"
+    (warp per 32 rows, for scattered columns)."""
+    k = C.c_int32()
+    _lib.check(_lib.load().nm_csr_spmv_kernel(A._h, C.byref(k)))
+    return {v: n for n, v in _KERNELS.items()}[k.value]
 
 
 def tune(A: CrsMatrix, tile: int = 0, max_rows: int = 0, short_max: int = 0,
-         grid_mult: int = -1, stages: int = 0) -> dict:
+         grid_mult: int = -1, stages: int = 0, kernel=None) -> dict:
     """Set the row-block partition parameters of A (tile / max_rows /
     short_max / stages <= 0 and grid_mult < 0 keep the current value;
-    grid_mult 0 is the automatic grid) and return the effective ones."""
-    t = _lib.Tuning(int(tile), int(max_rows), int(short_max), int(grid_mult), int(stages))
+    grid_mult 0 is the automatic grid) and its plain-SpMV kernel ("auto",
+    "blocks" or "gather"; None keeps it), and return the effective ones."""
+    if kernel is None:
+        k = 0
+    elif isinstance(kernel, str):
+        if kernel not in _KERNELS:
+            raise ValueError(f"kernel must be one of {sorted(_KERNELS)}, got {kernel!r}")
+        k = _KERNELS[kernel]
+    else:
+        k = int(kernel)
+    t = _lib.Tuning(int(tile), int(max_rows), int(short_max), int(grid_mult), int(stages), k)
     _lib.check(_lib.load().nm_csr_set_tuning(A._h, C.byref(t)), "tune")
     return tuning(A)
 
@@ -416,7 +437,8 @@ def _tune_key(A: CrsMatrix) -> str:
 def autotune(A: CrsMatrix, x=None, budget_ms: float = 200.0, cache: bool = True) -> dict:
     """Choose A's SpMV partition and launch shape by timing candidates on the
     device (nm_csr_autotune: tile 1024/2048/4096, short_max 32/64, stages
-    2/3/4, grid_mult 0/1/2) and install the fastest.  `x` (optional) is the
+    2/3/4, grid_mult 0/1/2 of the row-block kernel, and the warp-gather
+    kernel) and install the fastest.  `x` (optional) is the
     vector to time with, else U[-1, 1].  Results are cached per matrix
     signature in-process and, when NUM_B200_TUNE_CACHE names a JSON file,
     across processes.  Returns the installed tuning plus 'us' (its SpMV time)
@@ -424,7 +446,8 @@ def autotune(A: CrsMatrix, x=None, budget_ms: float = 200.0, cache: bool = True)
     import json
     import os
     path = os.environ.get("NUM_B200_TUNE_CACHE")
-    tune(A, tile=2048, max_rows=256, short_max=32, grid_mult=0, stages=2)  # key on defaults
+    tune(A, tile=2048, max_rows=256, short_max=32, grid_mult=0, stages=2,
+         kernel="auto")  # key on defaults
     key = _tune_key(A)
     if cache:
         if not _TUNE_CACHE and path and os.path.exists(path):
@@ -436,7 +459,7 @@ def autotune(A: CrsMatrix, x=None, budget_ms: float = 200.0, cache: bool = True)
         hit = _TUNE_CACHE.get(key)
         if hit:
             t = tune(A, **{k: hit[k] for k in ("tile", "max_rows", "short_max", "grid_mult",
-                                                "stages")})
+                                                "stages")}, kernel=hit.get("kernel", "auto"))
             return {**t, "us": hit.get("us"), "trials": [], "cached": True}
     dt = torch.float64 if A.precision == "fp64" else torch.float32
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -458,6 +481,7 @@ def autotune(A: CrsMatrix, x=None, budget_ms: float = 200.0, cache: bool = True)
     for t in trials[: min(cap, nt.value)]:
         out.append({"tile": t.tuning.tile, "short_max": t.tuning.short_max,
                     "stages": t.tuning.stages, "grid_mult": t.tuning.grid_mult,
+                    "kernel": {v: k for k, v in _KERNELS.items()}[t.tuning.kernel],
                     "us": round(float(t.us), 3)})
     res = tuning(A)
     us = min(o["us"] for o in out) if out else None

@@ -87,9 +87,12 @@ def test_reference_matrices_vs_scipy(kspmv, oracle, name):
     _check64(oracle, A, x, y, kspmv.row_blocks(M)[1])
 
 
-@pytest.mark.parametrize("tuning", [None, {"tile": 1024, "short_max": 8},
-                                    {"tile": 4096, "max_rows": 128, "short_max": 64},
-                                    {"grid_mult": 2}])
+# the row-block kernel (scattered columns would get the warp-gather kernel)
+@pytest.mark.parametrize("tuning", [{"kernel": "blocks"},
+                                    {"tile": 1024, "short_max": 8, "kernel": "blocks"},
+                                    {"tile": 4096, "max_rows": 128, "short_max": 64,
+                                     "kernel": "blocks"},
+                                    {"grid_mult": 2, "kernel": "blocks"}])
 def test_power_law_all_bins(kspmv, oracle, tuning):
     A = gen.power_law(200_000, seed=5)
     x = np.random.default_rng(1).uniform(-1, 1, A.ncols)
@@ -100,6 +103,82 @@ def test_power_law_all_bins(kspmv, oracle, tuning):
     assert np.array_equal(blk, oblk) and np.array_equal(bins, obins)  # device copy == oracle
     assert (bins == 1).any()
     _check64(oracle, A, x, y, bins)
+
+
+# ---- warp-gather kernel (scattered columns) ------------------------------------
+
+def test_gather_kernel_chosen_and_bit_exact(kspmv, oracle):
+    # power-law rows over 200,000 columns: no block has x windows, so spmv
+    # runs the warp-gather kernel, which sums every row serially
+    A = gen.power_law(200_000, seed=11)
+    x = np.random.default_rng(11).uniform(-1, 1, A.ncols)
+    y, M = _run(kspmv, A, x)
+    assert kspmv.spmv_kernel(M) == "gather" and kspmv.tuning(M)["kernel"] == "auto"
+    assert np.array_equal(y, oracle.spmv(A.row_ptr, A.col_idx, A.values, x))
+    y2, M2 = _run(kspmv, A, x, tuning={"kernel": "blocks"})
+    assert kspmv.spmv_kernel(M2) == "blocks"
+    _check64(oracle, A, x, y2, kspmv.row_blocks(M2)[1])
+
+
+def _scattered(nrows, lens_from, seed, ncols=1_000_000):
+    rng = np.random.default_rng(seed)
+    lens = rng.choice(lens_from, nrows)
+    lens[:: 7] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(ncols, l, replace=False)) if l else
+                         np.empty(0, np.int64) for l in lens]).astype(np.int32)
+    return gen.Csr(rp, ci, rng.standard_normal(rp[-1]), nrows, ncols), rng
+
+
+@pytest.mark.parametrize("nrows", [1, 31, 32, 33, 100, 1000])
+def test_gather_ragged_groups_and_empty_rows(kspmv, oracle, nrows):
+    # row groups cut at 32 rows, rows of 0 ... 4096 nonzeros over a million columns
+    A, rng = _scattered(nrows, [0, 1, 5, 40, 193, 300, 4096], nrows)
+    x = rng.uniform(-1, 1, A.ncols)
+    y, M = _run(kspmv, A, x)
+    if A.nnz:
+        assert kspmv.spmv_kernel(M) == "gather"
+    assert np.array_equal(y, oracle.spmv(A.row_ptr, A.col_idx, A.values, x))
+    assert np.all(y[np.diff(A.row_ptr) == 0] == 0.0)
+
+
+def test_gather_long_row_falls_back_and_forced(kspmv, oracle):
+    # a row longer than 4096 nonzeros keeps the row-block kernel under "auto";
+    # forced, the warp-gather kernel still sums it serially
+    A, rng = _scattered(200, [3, 17, 64, 5000], 5)
+    x = rng.uniform(-1, 1, A.ncols)
+    y, M = _run(kspmv, A, x)
+    assert kspmv.spmv_kernel(M) == "blocks"
+    _check64(oracle, A, x, y, kspmv.row_blocks(M)[1])
+    yg, Mg = _run(kspmv, A, x, tuning={"kernel": "gather"})
+    assert kspmv.spmv_kernel(Mg) == "gather"
+    assert np.array_equal(yg, oracle.spmv(A.row_ptr, A.col_idx, A.values, x))
+
+
+def test_gather_fp32_and_bf16_every_row_bit_exact(kspmv, oracle):
+    A = gen.power_law(100_000, seed=13)
+    x = np.random.default_rng(13).uniform(-1, 1, A.ncols).astype(np.float32)
+    y32, M = _run(kspmv, A, x, precision="fp32")
+    assert kspmv.spmv_kernel(M) == "gather"
+    assert np.array_equal(y32, oracle.spmv(A.row_ptr, A.col_idx, A.values.astype(np.float32), x))
+    yb, Mb = _run(kspmv, A, x, precision="bf16")
+    from num_b200.kokkos_spmv import _values_for
+    bits, _ = _values_for(A.values, "bf16")
+    vb = (bits.astype(np.uint32) << 16).view(np.float32)
+    assert kspmv.spmv_kernel(Mb) == "gather"
+    assert np.array_equal(yb, oracle.spmv(A.row_ptr, A.col_idx, vb, x))
+
+
+def test_tune_kernel_argument_errors(kspmv):
+    A = gen.tridiag4()
+    M = kspmv.upload_csr(*A.astuple())
+    with pytest.raises(ValueError):
+        kspmv.tune(M, kernel="fastest")
+    with pytest.raises(ValueError, match="kernel"):
+        kspmv.tune(M, kernel=7)
+    assert kspmv.tune(M, kernel="gather")["kernel"] == "gather"
+    assert kspmv.tune(M)["kernel"] == "gather"  # None keeps it
+    assert kspmv.tune(M, kernel="auto")["kernel"] == "auto"
 
 
 def test_ragged_long_and_empty_rows(kspmv, oracle):
@@ -257,8 +336,9 @@ def test_autotune_installs_a_valid_tuning(kspmv, oracle, tmp_path, monkeypatch):
     assert res["tile"] in (1024, 2048, 4096) and res["short_max"] in (32, 64)
     assert res["stages"] in (2, 3, 4) and res["grid_mult"] in (0, 1, 2)
     assert res["us"] == min(t["us"] for t in res["trials"])
-    assert {k: res[k] for k in ("tile", "short_max", "stages", "grid_mult")} == \
-        {k: kspmv.tuning(M)[k] for k in ("tile", "short_max", "stages", "grid_mult")}
+    assert {t["kernel"] for t in res["trials"]} == {"blocks", "gather"}
+    assert {k: res[k] for k in ("tile", "short_max", "stages", "grid_mult", "kernel")} == \
+        {k: kspmv.tuning(M)[k] for k in ("tile", "short_max", "stages", "grid_mult", "kernel")}
     xt = torch.tensor(x, device="cuda")
     yt = torch.full((A.nrows,), float("nan"), dtype=torch.float64, device="cuda")
     kspmv.spmv(M, xt, yt)
@@ -268,3 +348,4 @@ def test_autotune_installs_a_valid_tuning(kspmv, oracle, tmp_path, monkeypatch):
     kspmv._TUNE_CACHE.clear()
     again = kspmv.autotune(M, budget_ms=50)
     assert again["cached"] and again["tile"] == res["tile"] and again["stages"] == res["stages"]
+    assert again["kernel"] == res["kernel"]
