@@ -1,6 +1,8 @@
 // spmv.cu -- plain SpMV and multi-RHS SpMV kernels and their launchers.
 #include "spmv.cuh"
 
+#include <atomic>
+
 namespace nm {
 
 template <typename V, typename X, typename A, int TILE, int STAGES>
@@ -106,12 +108,13 @@ __global__ void __launch_bounds__(kGatherThreads)
 
 template <typename V, typename X, typename A>
 static int launch_gather(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    static int occ = 0;  // resident CTAs per SM (same on every device of the process)
+    static std::atomic<int> occ_cache{0};  // resident CTAs per SM (same on every device here)
+    int occ = occ_cache.load(std::memory_order_relaxed);
     if (occ == 0) {
-        int o = 0;
         NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &o, spmv_gather_kernel<V, X, A>, kGatherThreads, 0));
-        occ = o > 0 ? o : 1;
+            &occ, spmv_gather_kernel<V, X, A>, kGatherThreads, 0));
+        occ = occ > 0 ? occ : 1;
+        occ_cache.store(occ, std::memory_order_relaxed);
     }
     const int64_t groups = (int64_t(Am->nrows) + kGatherRows - 1) / kGatherRows;
     const int64_t need = (groups + kGatherThreads / 32 - 1) / (kGatherThreads / 32);
@@ -414,12 +417,13 @@ __global__ void __launch_bounds__(kBatchWarpThreads)
 template <int VEC, int CH>
 static int launch_batch_warp_t(const nm_csr* A, const double* X, double* Y, int32_t k,
                                cudaStream_t s) {
-    static int occ = 0;  // resident CTAs per SM (same on every device of the process)
+    static std::atomic<int> occ_cache{0};  // resident CTAs per SM (same on every device here)
+    int occ = occ_cache.load(std::memory_order_relaxed);
     if (occ == 0) {
-        int o = 0;
         NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &o, batch_spmv_warp_kernel<VEC, CH>, kBatchWarpThreads, 0));
-        occ = o > 0 ? o : 1;
+            &occ, batch_spmv_warp_kernel<VEC, CH>, kBatchWarpThreads, 0));
+        occ = occ > 0 ? occ : 1;
+        occ_cache.store(occ, std::memory_order_relaxed);
     }
     constexpr int warps = kBatchWarpThreads / 32;
     const int64_t need = (int64_t(A->nrows) + warps - 1) / warps;
