@@ -315,8 +315,9 @@ def spmv(A: CrsMatrix, x, y, kokkoskernels: bool = True, *, async_: bool = False
     """Single-GPU SpMV: y = A @ x (in place into y).
 
     `kokkoskernels` is accepted for compatibility; both settings run the
-    B200 row-block kernel (the reference's two backends compute the same
-    product).  fp32/bf16 matrices take float32 x and y."""
+    kernel chosen for A (spmv_kernel: the row-block pipeline or, for
+    scattered columns, the warp-gather kernel; the reference's two backends
+    compute the same product).  fp32/bf16 matrices take float32 x and y."""
     dt = _vec_dtype(A)
     xt = device_array(x, dt, "x")
     yt = device_array(y, dt, "y")
