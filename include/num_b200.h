@@ -391,6 +391,20 @@ int nm_halo_unpack(const nm_dist* D, const double* recv_buf, double* x_ext, void
  * x_ext, x_ext = [x_local | x_ghost].  With no ghosts x_ext may be x_local. */
 int nm_dist_spmv_local(const nm_dist* D, const double* x_ext, double* y_local, void* stream);
 
+/* The same product in two parts, so that the halo exchange can overlap the
+ * first (addition: the reference describes this overlap as future work,
+ * src/halo_exchange.hpp:28-33).  nm_dist_spmv_interior writes the rows whose
+ * columns are all owned, reading x_local only (no ghost needed, so it may run
+ * while the halo is in flight); nm_dist_spmv_boundary writes the other rows,
+ * reading x_ext = [x_local | x_ghost] after the unpack.  Together they write
+ * every row of y_local once, each row by the row-block kernel (rows of <= 32
+ * nonzeros summed serially in CSR order).  nm_dist_row_split reports the
+ * two row counts (also for host-only plans). */
+int nm_dist_spmv_interior(const nm_dist* D, const double* x_local, double* y_local,
+                          void* stream);
+int nm_dist_spmv_boundary(const nm_dist* D, const double* x_ext, double* y_local, void* stream);
+int nm_dist_row_split(const nm_dist* D, int32_t* n_interior, int32_t* n_boundary);
+
 /* cg_solve_distributed (src/cg_solver.hpp:38-125) at one rank (no ghosts):
  * CG of nm_cg_local plus the reference's breakdown guard |p.Ap| < 1e-300,
  * reported as NM_ERR_RUNTIME "CG: p'Ap is near zero - A may not be SPD". */

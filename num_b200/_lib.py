@@ -107,6 +107,9 @@ _SIGNATURES = {
     "nm_halo_pack": ([vp, vp, vp, vp], C.c_int),
     "nm_halo_unpack": ([vp, vp, vp, vp], C.c_int),
     "nm_dist_spmv_local": ([vp, vp, vp, vp], C.c_int),
+    "nm_dist_spmv_interior": ([vp, vp, vp, vp], C.c_int),
+    "nm_dist_spmv_boundary": ([vp, vp, vp, vp], C.c_int),
+    "nm_dist_row_split": ([vp, P_i32, P_i32], C.c_int),
     "nm_dist_cg_single": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
 }
 

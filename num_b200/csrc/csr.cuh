@@ -115,6 +115,9 @@ namespace nm {
 int spmv_grid(const nm_csr* A, int ctas_per_sm);
 // Launches y = A*x on `stream` (dtype-dispatched).  Used by the API and CG.
 int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t stream);
+// FP64 row-block SpMV of a row-subset matrix: y[rows[i]] = (A x)[i].
+int launch_spmv_rows(const nm_csr* A, const double* x, double* y, const int32_t* rows,
+                     cudaStream_t stream);
 // Dynamic shared memory of the SpMV kernel for (dtype, tile, stages); 0 if
 // the combination does not exist.
 size_t spmv_smem_for(int dtype, int tile, int stages);

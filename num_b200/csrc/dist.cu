@@ -30,9 +30,19 @@ struct nm_dist {
     std::vector<double> local_vals;
     nm_csr* local = nullptr;
     int32_t* d_send_idx = nullptr;
+    // Interior rows (every column owned) and boundary rows (some ghost
+    // column) as separate matrices, with their local row numbers, so the
+    // interior can be multiplied while the halo is exchanged.
+    int32_t n_interior = 0, n_boundary = 0;
+    nm_csr* interior = nullptr;   // columns in [0, local_n): reads x_local
+    nm_csr* boundary = nullptr;   // columns in [0, local_n + n_ghost): reads x_ext
+    int32_t* d_rows = nullptr;    // interior row numbers, then boundary row numbers
     ~nm_dist() {
         if (local) nm_csr_destroy(local);
+        if (interior) nm_csr_destroy(interior);
+        if (boundary) nm_csr_destroy(boundary);
         if (d_send_idx) cudaFree(d_send_idx);
+        if (d_rows) cudaFree(d_rows);
     }
 };
 
@@ -179,6 +189,20 @@ static int dist_build(const int32_t* rp, const int32_t* ci, const double* vals, 
     D->local_ci = std::move(lc);
     if (vals) D->local_vals.assign(vals + z0, vals + z1);
     else D->local_vals.assign(size_t(z1 - z0), 0.0);
+    // Interior / boundary split of the local rows (the overlap the reference
+    // describes as future work, src/halo_exchange.hpp:28-33).
+    std::vector<int32_t> rows_ib;  // interior rows, then boundary rows
+    {
+        std::vector<int32_t> brows;
+        for (int32_t r = 0; r < ln; ++r) {
+            bool ghost = false;
+            for (int32_t j = D->local_rp[r]; j < D->local_rp[r + 1]; ++j) ghost |= D->local_ci[j] >= ln;
+            (ghost ? brows : rows_ib).push_back(r);
+        }
+        D->n_interior = static_cast<int32_t>(rows_ib.size());
+        D->n_boundary = static_cast<int32_t>(brows.size());
+        rows_ib.insert(rows_ib.end(), brows.begin(), brows.end());
+    }
     if (!upload) {
         *out = D.release();
         return NM_OK;
@@ -187,6 +211,33 @@ static int dist_build(const int32_t* rp, const int32_t* ci, const double* vals, 
         int st = nm_csr_create(D->local_rp.data(), D->local_ci.data(), D->local_vals.data(),
                                NM_F64, ln, ln + D->n_ghost, &D->local);
         if (st != NM_OK) return st;
+    }
+    if (ln > 0 && D->n_ghost > 0) {
+        // the two row subsets as matrices of their own (rows in local order)
+        auto subset = [&](int32_t first, int32_t count, int32_t ncols_sub, nm_csr** outm) {
+            std::vector<int32_t> srp(1, 0), sci;
+            std::vector<double> sv;
+            for (int32_t k = first; k < first + count; ++k) {
+                const int32_t r = rows_ib[k];
+                for (int32_t j = D->local_rp[r]; j < D->local_rp[r + 1]; ++j) {
+                    sci.push_back(D->local_ci[j]);
+                    sv.push_back(D->local_vals[j]);
+                }
+                srp.push_back(static_cast<int32_t>(sci.size()));
+            }
+            return nm_csr_create(srp.data(), sci.data(), sv.data(), NM_F64, count, ncols_sub, outm);
+        };
+        if (D->n_interior > 0) {
+            int st = subset(0, D->n_interior, ln, &D->interior);
+            if (st != NM_OK) return st;
+        }
+        if (D->n_boundary > 0) {
+            int st = subset(D->n_interior, D->n_boundary, ln + D->n_ghost, &D->boundary);
+            if (st != NM_OK) return st;
+        }
+        NM_CUDA_TRY(cudaMalloc(&D->d_rows, sizeof(int32_t) * size_t(ln)));
+        NM_CUDA_TRY(cudaMemcpy(D->d_rows, rows_ib.data(), sizeof(int32_t) * size_t(ln),
+                               cudaMemcpyHostToDevice));
     }
     if (D->total_send > 0) {
         NM_CUDA_TRY(cudaMalloc(&D->d_send_idx, sizeof(int32_t) * size_t(D->total_send)));
@@ -307,6 +358,37 @@ extern "C" int nm_dist_spmv_local(const nm_dist* D, const double* x_ext, double*
     if (!D->local) return fail(NM_ERR_INVALID, "nm_dist_spmv_local: host-only plan handle");
     if (!x_ext || !y_local) return fail(NM_ERR_INVALID, "nm_dist_spmv_local: NULL vector");
     return nm::launch_spmv(D->local, x_ext, y_local, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int nm_dist_row_split(const nm_dist* D, int32_t* n_interior, int32_t* n_boundary) {
+    nm::clear_error();
+    if (!D) return fail(NM_ERR_INVALID, "nm_dist_row_split: NULL handle");
+    if (n_interior) *n_interior = D->n_interior;
+    if (n_boundary) *n_boundary = D->n_boundary;
+    return NM_OK;
+}
+
+extern "C" int nm_dist_spmv_interior(const nm_dist* D, const double* x_local, double* y_local,
+                                     void* stream) {
+    nm::clear_error();
+    if (!D) return fail(NM_ERR_INVALID, "nm_dist_spmv_interior: NULL handle");
+    if (D->row_end == D->row_start) return NM_OK;  // rank owns no rows
+    if (!D->local) return fail(NM_ERR_INVALID, "nm_dist_spmv_interior: host-only plan handle");
+    if (!x_local || !y_local) return fail(NM_ERR_INVALID, "nm_dist_spmv_interior: NULL vector");
+    auto s = static_cast<cudaStream_t>(stream);
+    if (D->n_ghost == 0) return nm::launch_spmv(D->local, x_local, y_local, s);  // all interior
+    if (!D->interior) return NM_OK;
+    return nm::launch_spmv_rows(D->interior, x_local, y_local, D->d_rows, s);
+}
+
+extern "C" int nm_dist_spmv_boundary(const nm_dist* D, const double* x_ext, double* y_local,
+                                     void* stream) {
+    nm::clear_error();
+    if (!D) return fail(NM_ERR_INVALID, "nm_dist_spmv_boundary: NULL handle");
+    if (D->row_end == D->row_start || D->n_ghost == 0 || !D->boundary) return NM_OK;
+    if (!x_ext || !y_local) return fail(NM_ERR_INVALID, "nm_dist_spmv_boundary: NULL vector");
+    return nm::launch_spmv_rows(D->boundary, x_ext, y_local, D->d_rows + D->n_interior,
+                                static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int nm_dist_cg_single(nm_dist* D, const double* b, double* x, double tol,

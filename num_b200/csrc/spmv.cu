@@ -142,6 +142,63 @@ static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     return NM_OK;
 }
 
+// y[rows[i]] = (A x)[i]: a matrix of some rows of a longer one, each row's
+// result written to its place in the longer y (the interior / boundary rows of
+// a distributed slice).
+struct MapStoreEpi {
+    static constexpr bool kBlockSums = false;
+    double* __restrict__ y;
+    const int32_t* __restrict__ rows;
+    __device__ __forceinline__ void operator()(int32_t row, double v) { y[__ldg(rows + row)] = v; }
+    __device__ __forceinline__ double take() { return 0.0; }
+    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+};
+
+template <int TILE, int STAGES>
+__global__ void __launch_bounds__(kCtaThreads)
+    spmv_rows_kernel(const CsrView<double> M, const double* __restrict__ x, double* y,
+                     const int32_t* rows, unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES>*>(smem_raw);
+    MapStoreEpi epi{y, rows};
+    spmv_pipeline<double, double, double, TILE, STAGES>(M, x, sm, epi, err);
+}
+
+template <int TILE, int STAGES>
+static int launch_rows_tile(const nm_csr* Am, const double* x, double* y, const int32_t* rows,
+                            cudaStream_t s) {
+    CsrView<double> M = Am->view<double>();
+    M.stage_x = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+    constexpr size_t smem = spmv_smem_bytes<double, double, double, TILE, STAGES>();
+    auto* fn = spmv_rows_kernel<TILE, STAGES>;
+    int occ = 0;
+    int st = prepare_kernel(reinterpret_cast<const void*>(fn), kCtaThreads, smem, &occ);
+    if (st != NM_OK) return st;
+    unsigned int* err = device_error_word();
+    if (!err) return fail(NM_ERR_CUDA, "spmv: cannot map the device error word");
+    fn<<<spmv_grid(Am, occ), kCtaThreads, smem, s>>>(M, x, y, rows, err);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+template <int TILE>
+static int launch_rows_stages(const nm_csr* Am, const double* x, double* y, const int32_t* rows,
+                              cudaStream_t s) {
+    if (Am->tune.stages == 4) return launch_rows_tile<TILE, 4>(Am, x, y, rows, s);
+    if (Am->tune.stages == 3) return launch_rows_tile<TILE, 3>(Am, x, y, rows, s);
+    return launch_rows_tile<TILE, 2>(Am, x, y, rows, s);
+}
+
+int launch_spmv_rows(const nm_csr* A, const double* x, double* y, const int32_t* rows,
+                     cudaStream_t s) {
+    if (A->dtype != NM_F64) return fail(NM_ERR_TYPE, "spmv_rows: float64 matrices only");
+    switch (A->tune.tile) {
+        case 1024: return launch_rows_stages<1024>(A, x, y, rows, s);
+        case 4096: return launch_rows_stages<4096>(A, x, y, rows, s);
+        default: return launch_rows_stages<2048>(A, x, y, rows, s);
+    }
+}
+
 template <typename V, typename X, typename A, int TILE>
 static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     if (Am->tune.stages == 4) return launch_tile<V, X, A, TILE, 4>(Am, x, y, s);

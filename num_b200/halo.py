@@ -12,7 +12,11 @@ GPU over torch.distributed:
     messages match by (peer, order) as the reference's tag-42 Isend/Irecv do;
   * unpack: the library kernel writes the received values behind the owned
     entries of x_ext = [x_local | x_ghost];
-  * SpMV on x_ext with the remapped local matrix.
+  * SpMV on x_ext with the remapped local matrix -- on GPUs in two parts:
+    the rows whose columns are all owned are multiplied from x_local while
+    the exchange is in flight, the rows with ghost columns after the unpack
+    (the overlap the reference describes as future work,
+    src/halo_exchange.hpp:28-33).
 
 With one rank there are no ghosts: dist_spmv is the local SpMV on x_local
 directly (the reference still allocates and fills x_ext per call, which is
@@ -108,17 +112,27 @@ def plan_host(rowptr, colind, values, n: int, ncols: int, rank: int, size: int):
     return plan, (lrp, lci, lv)
 
 
-def exchange(plan: HaloPlan, send_buf, recv_buf, group=None) -> None:
-    """Send each neighbour its packed segment and receive each owner's ghost
-    segment (src/halo_exchange.hpp:237-285), as one batch of P2P ops."""
+def exchange_start(plan: HaloPlan, send_buf, recv_buf, group=None) -> list:
+    """Post the exchange (src/halo_exchange.hpp:237-285): each neighbour's
+    packed segment sent, each owner's ghost segment received, as one batch of
+    P2P ops.  Returns the requests for exchange_wait."""
     ops = []
     for r, c, o in zip(plan.recv_rank, plan.recv_count, plan.recv_off):
         ops.append(dist.P2POp(dist.irecv, recv_buf[int(o):int(o) + int(c)], int(r), group))
     for r, c, o in zip(plan.send_rank, plan.send_count, plan.send_off):
         ops.append(dist.P2POp(dist.isend, send_buf[int(o):int(o) + int(c)], int(r), group))
-    if ops:
-        for req in dist.batch_isend_irecv(ops):
-            req.wait()
+    return dist.batch_isend_irecv(ops) if ops else []
+
+
+def exchange_wait(reqs) -> None:
+    """Complete the exchange (with NCCL: the current stream waits for it)."""
+    for req in reqs:
+        req.wait()
+
+
+def exchange(plan: HaloPlan, send_buf, recv_buf, group=None) -> None:
+    """The whole halo exchange: exchange_start then exchange_wait."""
+    exchange_wait(exchange_start(plan, send_buf, recv_buf, group))
 
 
 class DeviceOps:
@@ -145,14 +159,19 @@ class DeviceOps:
             _lib.check(self.lib.nm_dist_spmv_local(self.A._h, x.data_ptr(), y.data_ptr(),
                                                    self._s()), "dist_spmv")
             return
-        self.x_ext[: p.local_n].copy_(x)  # x_ext_fill_local (src/dist_spmv.hpp:139-142)
         _lib.check(self.lib.nm_halo_pack(self.A._h, x.data_ptr(), self.send_buf.data_ptr(),
                                          self._s()), "halo_pack")
-        exchange(p, self.send_buf, self.recv_buf, self.group)
+        reqs = exchange_start(p, self.send_buf, self.recv_buf, self.group)
+        # while the halo is in flight: the rows without ghost columns, and the
+        # owned part of x_ext (x_ext_fill_local, src/dist_spmv.hpp:139-142)
+        _lib.check(self.lib.nm_dist_spmv_interior(self.A._h, x.data_ptr(), y.data_ptr(),
+                                                  self._s()), "dist_spmv")
+        self.x_ext[: p.local_n].copy_(x)
+        exchange_wait(reqs)
         _lib.check(self.lib.nm_halo_unpack(self.A._h, self.recv_buf.data_ptr(),
                                            self.x_ext.data_ptr(), self._s()), "halo_unpack")
-        _lib.check(self.lib.nm_dist_spmv_local(self.A._h, self.x_ext.data_ptr(), y.data_ptr(),
-                                               self._s()), "dist_spmv")
+        _lib.check(self.lib.nm_dist_spmv_boundary(self.A._h, self.x_ext.data_ptr(), y.data_ptr(),
+                                                  self._s()), "dist_spmv")
 
     def dot(self, x, y) -> float:
         out = C.c_double()

@@ -108,6 +108,27 @@ def test_dist_plan_bit_exact(nmlib, oracle, name, A, P):
         assert np.array_equal(lv, o["values"])
 
 
+@pytest.mark.parametrize("name,A,P", list(_plans()), ids=[p[0] for p in _plans()])
+def test_dist_row_split_counts(nmlib, name, A, P):
+    """Interior rows (every column owned) and boundary rows (a ghost column)
+    of each rank's slice, counted on a host-only plan."""
+    from num_b200.halo import plan_host
+    for r in range(P):
+        plan, (lrp, lci, _) = plan_host(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols, r, P)
+        h = C.c_void_p()
+        from num_b200._lib import check as _lib_check
+        _lib_check(nmlib.nm_dist_plan(A.row_ptr.ctypes.data, A.col_idx.ctypes.data,
+                                      A.values.ctypes.data, A.nrows, A.ncols, r, P, C.byref(h)))
+        ni, nb = C.c_int32(), C.c_int32()
+        try:
+            _lib_check(nmlib.nm_dist_row_split(h, C.byref(ni), C.byref(nb)))
+        finally:
+            nmlib.nm_dist_destroy(h)
+        n = plan.row_end - plan.row_start
+        ghost = np.array([bool((lci[lrp[i]:lrp[i + 1]] >= n).any()) for i in range(n)], bool)
+        assert (ni.value, nb.value) == (int((~ghost).sum()), int(ghost.sum()))
+
+
 def test_dist_plan_rejects_out_of_range_column(nmlib):
     from num_b200.halo import plan_host
     # Row 1 (owned by rank 1 of 2) names column 5 of a 2-row matrix; rank 1's

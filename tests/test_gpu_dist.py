@@ -39,14 +39,19 @@ class VirtualRank:
         _lib.load().nm_dist_destroy(self.h)
 
 
-def dist_spmv_virtual(ranks, x):
+def dist_spmv_virtual(ranks, x, split=False):
+    """split: each rank multiplies its interior rows from x_local before the
+    exchange and its boundary rows from x_ext after it (the overlapped
+    order); else the whole slice after the exchange."""
     lib = _lib.load()
     s = torch.cuda.current_stream().cuda_stream
-    for vr in ranks:  # fill local part + pack
+    for vr in ranks:  # fill local part + pack (+ interior rows)
         p = vr.plan
         xl = torch.tensor(x[p.row_start:p.row_end], device="cuda")
         vr.x_ext[: p.local_n].copy_(xl)
         _lib.check(lib.nm_halo_pack(vr.h, xl.data_ptr(), vr.send.data_ptr(), s))
+        if split:
+            _lib.check(lib.nm_dist_spmv_interior(vr.h, xl.data_ptr(), vr.y.data_ptr(), s))
     for vr in ranks:  # loopback exchange: owner q's segment for r -> r's recv buffer
         p = vr.plan
         for q, cnt, off in zip(p.recv_rank, p.recv_count, p.recv_off):
@@ -58,7 +63,10 @@ def dist_spmv_virtual(ranks, x):
     out = []
     for vr in ranks:
         _lib.check(lib.nm_halo_unpack(vr.h, vr.recv.data_ptr(), vr.x_ext.data_ptr(), s))
-        _lib.check(lib.nm_dist_spmv_local(vr.h, vr.x_ext.data_ptr(), vr.y.data_ptr(), s))
+        if split:
+            _lib.check(lib.nm_dist_spmv_boundary(vr.h, vr.x_ext.data_ptr(), vr.y.data_ptr(), s))
+        else:
+            _lib.check(lib.nm_dist_spmv_local(vr.h, vr.x_ext.data_ptr(), vr.y.data_ptr(), s))
         out.append(vr.y[: vr.plan.local_n].cpu().numpy())
     return np.concatenate(out)
 
@@ -87,6 +95,27 @@ def test_virtual_rank_dist_spmv(kspmv, oracle, P, name, make, seed):
                                   oracle.halo_pack(part["send_idx"], xl))
     ref = A.to_scipy() @ x
     assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 7])
+@pytest.mark.parametrize("name,make,seed", CASES, ids=[c[0] for c in CASES])
+def test_virtual_rank_interior_boundary_split(kspmv, oracle, P, name, make, seed):
+    # interior rows before the exchange + boundary rows after it == the
+    # whole-slice product, bit for bit, and the oracle's distributed SpMV
+    A = make()
+    x = np.random.default_rng(seed).standard_normal(A.nrows)
+    ranks = [VirtualRank(A, r, P) for r in range(P)]
+    y_split = dist_spmv_virtual(ranks, x, split=True)
+    y_whole = dist_spmv_virtual(ranks, x)
+    assert np.array_equal(y_split, y_whole)
+    parts = oracle.partition(A.row_ptr, A.col_idx, A.values, A.nrows, P)
+    assert np.array_equal(y_split, oracle.dist_spmv(parts, x))
+    lib = _lib.load()
+    for vr in ranks:
+        ni, nb = C.c_int32(), C.c_int32()
+        _lib.check(lib.nm_dist_row_split(vr.h, C.byref(ni), C.byref(nb)))
+        assert ni.value + nb.value == vr.plan.local_n
+        assert (nb.value == 0) == (vr.plan.n_ghost == 0)
 
 
 def test_virtual_rank_zero_and_basis(kspmv):
