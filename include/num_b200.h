@@ -245,7 +245,7 @@ typedef struct nm_solver nm_solver;
 /* Solver options.  inner: value precision of the inner iterations -- NM_F64
  * (plain FP64 Jacobi-PCG, no refinement), NM_F32 or NM_BF16 (FP32 vectors and
  * accumulation, FP64 iterative refinement).  precond: 1 Jacobi, 0 none.
- * inner_rtol: relative reduction of one inner solve (default 1e-4; ignored
+ * inner_rtol: relative reduction of one inner solve (default 1e-3; ignored
  * for NM_F64).  max_outer: refinement steps before giving up (default 30). */
 typedef struct {
     int32_t inner;

@@ -708,7 +708,7 @@ struct nm_solver {
     int device = 0;
     int inner = NM_F32;  // inner value precision: NM_F64 (plain PCG), NM_F32 or NM_BF16
     int precond = 1;
-    double inner_rtol = 1e-4;
+    double inner_rtol = 1e-3;
     int max_outer = 30;
     int64_t cap_rows = 0, cap_nnz = 0;
     int32_t cap_sys = 0;

@@ -44,7 +44,7 @@ def arena_for(budget_bytes: int, nnz_per_row: float = 8.0, precision: str = "fp3
 
 class BatchSolver:
     def __init__(self, max_rows: int, max_nnz: int, max_systems: int = 4096,
-                 precision: str = "fp32", precond: str = "jacobi", inner_rtol: float = 1e-4,
+                 precision: str = "fp32", precond: str = "jacobi", inner_rtol: float = 1e-3,
                  max_outer: int = 30, device: int = 0):
         import torch
         torch.cuda.set_device(device)
