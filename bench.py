@@ -939,17 +939,21 @@ def secondary(local_rank):
                                "e2e_solves_per_s": round(1e3 / r["e2e_ms"], 2)}
     out["setup_c2a"] = setup_c2a_measure(dev)
     requests = serve.make_requests(200, rate=0.0, seed=4)
-    s = serve_measure(dev, requests, 1, 1, 64e9)
-    st = s["stats"][0]
+    # two timed passes on each side, the better one of each (host wall clock
+    # of the pass, as serve / serve_plain report it)
+    s = serve_measure(dev, requests, 2, 2, 64e9)
+    st = max(s["stats"], key=lambda r: r["solves_per_s"])
     out["serve_c5_sample"] = {
         "requests": 200, "arrivals": "all at t=0 (saturated)",
-        "served_fp32_ir_solves_per_s": round(200 / (s["ms"] * 1e-3), 2),
+        "served_fp32_ir_solves_per_s": round(st["solves_per_s"], 2),
+        "served_passes": [round(r["solves_per_s"], 3) for r in s["stats"]],
         "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
         "plain_fp64_solves_per_s": round(s["plain"]["solves_per_s"], 2),
         "plain_passes": s["plain"]["passes_solves_per_s"],
         "plain_p50_ms": round(s["plain"]["p50_ms"], 2),
         "plain_p99_ms": round(s["plain"]["p99_ms"], 2),
-        "ratio_vs_plain": round(200 / (s["ms"] * 1e-3) / s["plain"]["solves_per_s"], 3),
+        "ratio_vs_plain": round(st["solves_per_s"] / s["plain"]["solves_per_s"], 3),
+        "comparison": "the better of two passes on each side",
         "max_true_residual_fp64": s["max_true_residual"]}
     return out
 
