@@ -252,6 +252,9 @@ typedef struct {
     int32_t precond;
     double inner_rtol;
     int32_t max_outer;
+    double cont_window; /* a refinement step keeps the Krylov direction while the
+                           true residual is within this factor of the inner
+                           solve's estimate (default 2; <= 0 keeps the default) */
 } nm_solver_opts;
 
 /* A solver with a device arena for up to max_rows rows and max_nnz nonzeros

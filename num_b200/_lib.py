@@ -28,7 +28,7 @@ class CgResult(C.Structure):
 
 class SolverOpts(C.Structure):
     _fields_ = [("inner", C.c_int32), ("precond", C.c_int32), ("inner_rtol", C.c_double),
-                ("max_outer", C.c_int32)]
+                ("max_outer", C.c_int32), ("cont_window", C.c_double)]
 
 
 class Tuning(C.Structure):

@@ -54,7 +54,7 @@ enum SysPhase : int32_t { kSysFree = 0, kSysOuter = 1, kSysInner = 2, kSysDone =
 struct SysState {
     // set at admission
     int32_t row0, n, max_iter, max_outer;
-    double tol, bnorm, inner_rtol, stop_frac;
+    double tol, bnorm, inner_rtol, stop_frac, cont_window;
     // dynamic
     int32_t phase, it_total, it_inner, outer;
     int32_t converged, pad_;
@@ -287,13 +287,14 @@ __global__ void __launch_bounds__(kScalarThreads)
                 // beta of unscaled CG times the scale change (s_new / s_old):
                 // (s_new / s_old) (r.z)_new / (r.z)_last.  Only while the
                 // recurrence still tracks the true residual (the new |b - Ax|
-                // within 2x of the inner solve's estimate rnorm_prev |r|);
+                // within a factor cont_window, 2 by default, of the inner
+                // solve's estimate rnorm_prev |r|);
                 // when it does not (low-precision values, ill conditioning)
                 // the inner solve restarts from p = z.
                 const double est = S.rnorm_prev * sqrt(S.rr);
                 const bool cont = S.outer >= 2 && S.rz_keep > 0.0 && S.rnorm_prev > 0.0 &&
-                                  t.x > 0.0 && est > 0.0 && S.rnorm <= 2.0 * est &&
-                                  S.rnorm >= 0.5 * est;
+                                  t.x > 0.0 && est > 0.0 && S.rnorm <= S.cont_window * est &&
+                                  S.rnorm * S.cont_window >= est;
                 S.gamma = cont ? (S.rnorm / S.rnorm_prev) * (t.x / S.rz_keep) : 0.0;
                 S.rzp[0] = t.x;
                 S.rzp[1] = t.x;
@@ -710,6 +711,7 @@ struct nm_solver {
     int precond = 1;
     double inner_rtol = 1e-3;
     int max_outer = 30;
+    double cont_window = 2.0;
     int64_t cap_rows = 0, cap_nnz = 0;
     int32_t cap_sys = 0;
     nm::RangeAlloc rows, nnz;
@@ -1072,6 +1074,7 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
         S->precond = opts->precond;
         if (opts->inner_rtol > 0) S->inner_rtol = opts->inner_rtol;
         if (opts->max_outer > 0) S->max_outer = opts->max_outer;
+        if (opts->cont_window > 0) S->cont_window = opts->cont_window;
     }
     if (S->inner != NM_F64 && S->inner != NM_F32 && S->inner != NM_BF16)
         return fail(NM_ERR_TYPE, "nm_solver_create: unknown inner precision %d", S->inner);
@@ -1369,6 +1372,7 @@ void job_prep(const nm_solver* S, AdmitJob& J, bool inner_threads) {
     ss->bnorm = bb > 0.0 ? std::sqrt(bb) : 1.0;
     ss->inner_rtol = S->inner == NM_F64 ? 0.0 : S->inner_rtol;
     ss->stop_frac = S->inner == NM_F64 ? 1.0 : 0.5;
+    ss->cont_window = S->cont_window;
     ss->phase = kSysOuter;
 }
 

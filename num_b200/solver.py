@@ -45,7 +45,7 @@ def arena_for(budget_bytes: int, nnz_per_row: float = 8.0, precision: str = "fp3
 class BatchSolver:
     def __init__(self, max_rows: int, max_nnz: int, max_systems: int = 4096,
                  precision: str = "fp32", precond: str = "jacobi", inner_rtol: float = 1e-3,
-                 max_outer: int = 30, device: int = 0):
+                 max_outer: int = 30, device: int = 0, cont_window: float = 2.0):
         import torch
         torch.cuda.set_device(device)
         if precision not in _PREC:
@@ -53,7 +53,7 @@ class BatchSolver:
         self.lib = _lib.load()
         _lib.check(self.lib.nm_init(device, None, None), "init")
         opts = _lib.SolverOpts(_PREC[precision], 1 if precond == "jacobi" else 0,
-                               float(inner_rtol), int(max_outer))
+                               float(inner_rtol), int(max_outer), float(cont_window))
         h = C.c_void_p()
         _lib.check(self.lib.nm_solver_create(int(max_rows), int(max_nnz), int(max_systems),
                                              C.byref(opts), C.byref(h)), "nm_solver_create")
