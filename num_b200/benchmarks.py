@@ -112,16 +112,23 @@ def _gpu_ready():
         return False
 
 
+_OWN_GROUP = []  # the process group this module created (destroyed by main)
+
+
 def _init_ranks():
     """(rank, size, kspmv or None): the drop-in module on this rank's GPU
     (rank % GPUs, as the reference scripts assign devices)."""
     import os
+    from datetime import timedelta
     rank, size = 0, 1
     if not _gpu_ready():
         return rank, size, None
     import torch
     if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not torch.distributed.is_initialized():
-        torch.distributed.init_process_group("nccl")
+        # a short timeout: a rank that stops answering ends the others' next
+        # collective with an error instead of a long hang
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=120))
+        _OWN_GROUP.append(True)
     from . import kokkos_spmv as kspmv
     if torch.distributed.is_initialized():
         rank, size = torch.distributed.get_rank(), torch.distributed.get_world_size()
@@ -314,7 +321,13 @@ def main(argv=None) -> int:
     if not argv or argv[0] not in ("spmv", "cg"):
         print("usage: python -m num_b200.benchmarks {spmv,cg} [options]", file=sys.stderr)
         return 2
-    (run_spmv if argv[0] == "spmv" else run_cg)(argv[1:])
+    try:
+        (run_spmv if argv[0] == "spmv" else run_cg)(argv[1:])
+    finally:
+        if _OWN_GROUP:
+            import torch
+            torch.distributed.destroy_process_group()
+            _OWN_GROUP.clear()
     return 0
 
 
