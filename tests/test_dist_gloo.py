@@ -30,20 +30,44 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _row_subset(rp, ci, v, rows):
+    """CSR of the given rows of (rp, ci, v), rows in the given order."""
+    lens = (rp[rows + 1] - rp[rows]).astype(np.int64)
+    srp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    take = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows]) if len(rows) else \
+        np.empty(0, np.int64)
+    return srp, ci[take].astype(np.int32), v[take]
+
+
 class CpuOps:
-    """Oracle-backed stand-ins for DeviceOps (same interface)."""
+    """Oracle-backed stand-ins for DeviceOps (same interface and the same
+    overlapped order: the exchange is posted, the rows without ghost columns
+    are multiplied from x_local, then the exchange completes and the rows with
+    ghost columns are multiplied from x_ext)."""
 
     def __init__(self, plan, local_csr, oracle, halo):
         self.plan, self.csr, self.o, self.halo = plan, local_csr, oracle, halo
         self.send = torch.zeros(max(plan.total_send, 1), dtype=torch.float64)
         self.recv = torch.zeros(max(plan.n_ghost, 1), dtype=torch.float64)
+        rp, ci, v = local_csr
+        n = plan.local_n
+        ghost = np.array([bool((ci[rp[i]:rp[i + 1]] >= n).any()) for i in range(n)], bool)
+        self.irows, self.brows = np.flatnonzero(~ghost), np.flatnonzero(ghost)
+        self.icsr = _row_subset(rp, ci, v, self.irows)
+        self.bcsr = _row_subset(rp, ci, v, self.brows)
 
     def spmv(self, x, y):
         p = self.plan
         self.send[: p.total_send] = torch.from_numpy(self.o.halo_pack(p.send_idx, x.numpy()))
-        self.halo.exchange(p, self.send, self.recv)
-        x_ext = np.concatenate([x.numpy(), self.recv[: p.n_ghost].numpy()])
-        y.copy_(torch.from_numpy(self.o.spmv(*self.csr, x_ext)))
+        reqs = self.halo.exchange_start(p, self.send, self.recv)
+        out = np.empty(p.local_n)
+        if len(self.irows):  # while the halo is in flight
+            out[self.irows] = self.o.spmv(*self.icsr, x.numpy())
+        self.halo.exchange_wait(reqs)
+        if len(self.brows):
+            x_ext = np.concatenate([x.numpy(), self.recv[: p.n_ghost].numpy()])
+            out[self.brows] = self.o.spmv(*self.bcsr, x_ext)
+        y.copy_(torch.from_numpy(out))
 
     def dot(self, x, y):
         return self.o.dot(x.numpy(), y.numpy())
