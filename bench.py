@@ -737,6 +737,14 @@ def run_engine(args, rank, world, local_rank):
     for _ in range(e_steps):
         (xe, ie), = S.solve([(A, b)], tol=1e-10, max_iter=20000, chunk=chunk)
     e_ms = (time.perf_counter() - e0) * 1e3 / e_steps
+    err_fp64 = None
+    if precision != "fp64":
+        # untimed: the same system by the FP64 engine, the reference solution
+        # the mixed-precision result is compared with
+        R = BatchSolver(A.nrows + 4096, A.nnz + 4096, 4, precision="fp64")
+        (x64, _), = R.solve([(A, b)], tol=1e-10, max_iter=20000, chunk=chunk)
+        err_fp64 = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
+        del R
     barrier(world)
     ms, e_ms = max_over_ranks([ms, e_ms], world, dev)
     if rank != 0:
@@ -755,6 +763,7 @@ def run_engine(args, rank, world, local_rank):
               "tol": 1e-10, "inner_iterations": st["iters"], "outer_steps": outer,
               "iterations_enqueued_per_solve": its, "residual": st["residual"],
               "true_residual_fp64": true_res, "converged": st["converged"],
+              "rel_error_vs_fp64_solution": err_fp64,
               "chunk": chunk, "parallelism": f"replicas x{world}",
               "api": "num_b200.solver.BatchSolver (C ABI nm_solver_*): admit once, "
                      "nm_solver_resolve + steps per solve",
@@ -798,10 +807,12 @@ def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, loc
     S = BatchSolver(rows, nnz, 1024, precision="fp32")
     ext = torch.cuda.ExternalStream(S.stream(), device=dev)
     errs = []
+    sols = {}
 
     def check_fn(i, x, info):
         _, A, b, _ = requests[i]
         errs.append(float(np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)))
+        sols[i] = np.array(x, copy=True)
 
     # untimed: one pass that checks every result's true FP64 residual, and the
     # warm-up passes
@@ -829,6 +840,15 @@ def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, loc
         pst = max(runs, key=lambda r: r["solves_per_s"])
         pst["passes_solves_per_s"] = [round(r["solves_per_s"], 3) for r in runs]
         out["plain"] = pst
+        # untimed: every served (FP32 + refinement) result against the plain
+        # FP64 drop-in's solution of the same request
+        rel = []
+
+        def cmp_fn(i, x, info):
+            if i in sols:
+                rel.append(float(np.linalg.norm(sols[i] - x) / max(np.linalg.norm(x), 1e-300)))
+        serve.serve_plain(requests, tol=1e-8, check=cmp_fn)
+        out["max_rel_error_vs_fp64"] = max(rel) if rel else None
     return out
 
 
@@ -860,6 +880,7 @@ def run_serve(args, rank, world, local_rank):
               "rows_total": tot_rows, "nnz_total": tot_nnz, "tol": 1e-8,
               "arena_gb_cap": args.arena_gb, "inner": "fp32 values + vectors, FP64 refinement",
               "max_true_residual_fp64": r["max_true_residual"],
+              "max_rel_error_vs_fp64_dropin": r.get("max_rel_error_vs_fp64"),
               "parallelism": f"replicas x{world}",
               "api": "num_b200.serve.serve over BatchSolver (nm_solver_* C ABI)"}
     line = base_line(args, world, round(world * solves_s, 3), "solves/s", ms_per, precision,
@@ -954,7 +975,8 @@ def secondary(local_rank):
         "plain_p99_ms": round(s["plain"]["p99_ms"], 2),
         "ratio_vs_plain": round(st["solves_per_s"] / s["plain"]["solves_per_s"], 3),
         "comparison": "the better of two passes on each side",
-        "max_true_residual_fp64": s["max_true_residual"]}
+        "max_true_residual_fp64": s["max_true_residual"],
+        "max_rel_error_vs_fp64_dropin": s.get("max_rel_error_vs_fp64")}
     return out
 
 
