@@ -187,3 +187,17 @@ def test_python_module_errors_on_host(nmlib):
         k.upload_csr(A.row_ptr, A.col_idx[:5], A.values, 4, 4)
     with pytest.raises(ValueError, match="outside"):
         k.upload_csr(A.row_ptr, A.col_idx, A.values, 4, 3)  # column 3 >= ncols
+
+
+def test_tune_kernel_names_checked_on_host(nmlib):
+    """kokkos_spmv.tune(kernel=...) validates the name before any device call;
+    the names map to nm_tuning.kernel as the header defines them."""
+    from num_b200 import kokkos_spmv as k
+    with pytest.raises(ValueError, match="kernel must be one of"):
+        k.tune(None, kernel="fastest")
+    assert k._KERNELS == {"auto": 1, "blocks": 2, "gather": 3}
+    t = C.c_int32()
+    st = nmlib.nm_csr_spmv_kernel(None, C.byref(t))
+    from num_b200 import _lib
+    assert st == _lib.NM_ERR_INVALID
+
