@@ -225,8 +225,13 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * serving engine that reserves nearly all of HBM), and latency-critical loops
  * where cudaMalloc / cudaFree would synchronise the device.  Same algorithm,
  * kernels and result as nm_cg_local, but every scratch vector comes from one
- * fixed device array that is part of the library (about 6.3 MB held by every
- * GPU that loads the library, until exit) instead of a per-matrix workspace.
+ * fixed device array that is part of the library (about 6.3 MB, held until
+ * exit) instead of a per-matrix workspace.  The driver reserves that array
+ * on a device when it loads the CG code there: under CUDA's default lazy
+ * module loading that is the first call of nm_cg_local_static or nm_cg_local
+ * on the device (with CUDA_MODULE_LOADING=EAGER, when the library loads), so
+ * a caller whose pool will claim nearly all of HBM makes one call (a solve
+ * of any small matrix) on each device before that pool takes its memory.
  * A is a handle made earlier with nm_csr_create; b, x as in nm_cg_local.
  * Limit: A->nrows <= 262,144 (larger matrices: NM_ERR_INVALID).  The first
  * call on a device looks up the array's device address, and the first call
@@ -234,7 +239,7 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * first calls before any stream capture.  All calls
  * share the one array (the state is reset at the start of each call); calls
  * that overlap on the GPU would race, so this entry point serialises its host
- * callers and synchronises `stream` before returning. */
+ * callers and synchronises `stream` before returning, on error returns too. */
 int nm_cg_local_static(const nm_csr* A, const double* b, double* x, double tol,
                        int32_t max_iter, nm_cg_result* result, void* stream);
 

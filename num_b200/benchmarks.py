@@ -16,10 +16,11 @@ Backends: scipy (scipy_cpu / scipy_cg), kokkos (kokkos_kk_1gpu), kokkos_custom
 (kokkos_custom_1gpu; the same B200 kernels), kokkos_dist (ranks of a
 torch.distributed job), batch (kokkos_batch_k<k>).  jax, petsc and the
 mpi4py launch are not installed here; their rows are reported as skipped.
-Matrices: laplacian_2d and laplacian_3d, sized from --N as the reference's
-registry does (matrix_generators.py:226-230: L = int(N**0.5),
-L = round(N**(1/3))).  The reference's lattice_gauge, random_sparse and
-power_law generators are not provided.
+Matrices: the reference registry's five (matrix_generators.py:234-260):
+laplacian_2d, laplacian_3d, lattice_gauge, random_sparse and power_law, sized
+from --N as it does (L = int(N**0.5) for the 2-D grids, round(N**(1/3)) for
+the 3-D one, N rows for the others), with the same arrays
+(num_b200.generators).
 CSV files go to --out (default ./benchmark_results), named spmv_<time>.csv /
 cg_<time>.csv like the reference's.
 """
@@ -34,18 +35,15 @@ from pathlib import Path
 
 import numpy as np
 
-MATRICES = ("laplacian_2d", "laplacian_3d")
+from .generators import MATRICES
+
 SKIPPED_BACKENDS = {"jax": "jax is not installed", "petsc": "petsc4py is not installed"}
 
 
 def get_matrix(name: str, N: int):
-    """The reference registry's sizing of its Laplacians (a host CSR)."""
+    """The reference registry's matrices and sizing (a host CSR)."""
     from . import generators as gen
-    if name == "laplacian_2d":
-        return gen.laplacian_2d(int(N ** 0.5))
-    if name == "laplacian_3d":
-        return gen.laplacian_3d(int(round(N ** (1.0 / 3.0))))
-    raise ValueError(f"matrix {name!r} is not available here; choose from {list(MATRICES)}")
+    return gen.get_matrix(name, N)
 
 
 def spmv_metrics(elapsed_s: float, N: int, nnz: int, k: int = 1) -> dict:

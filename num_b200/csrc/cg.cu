@@ -734,8 +734,15 @@ extern "C" int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, in
 // device and stall every other stream.  nm_cg_local caches a workspace per
 // matrix, allocated on first use; this variant instead takes r, p, Ap, the
 // CTA partial sums, the device-resident CG state and the error word from one
-// file-scope device array that is part of the loaded library (every GPU that
-// loads the library holds it, about 6.3 MB, until the process exits).
+// file-scope device array that is part of the loaded library (about 6.3 MB,
+// held until the process exits by every GPU on which this file's module has
+// been loaded).  Under CUDA's default lazy module loading the driver loads the
+// module, and so reserves the array, on the first use of this file's kernels
+// or symbols on a device -- normally the first call of this entry point or of
+// nm_cg_local there; with CUDA_MODULE_LOADING=EAGER it happens when the
+// library is loaded.  A caller whose own pool will claim nearly all of HBM
+// makes one call (a solve of any small matrix) on each device before that
+// pool takes its memory.
 //
 // It runs the same kernels in the same order with the same grids as
 // nm_cg_local (launched directly instead of through cached CUDA graphs, and
@@ -849,6 +856,19 @@ int static_attr_stages(int stages, int* occ) {
     return stages == 3 ? static_attr<TILE, 3>(occ) : static_attr<TILE, 2>(occ);
 }
 
+// Waits for `s` when it goes out of scope, whatever the return path, once
+// armed.  Declared after the lock, so it runs before the lock is released: a
+// call that fails after enqueueing work leaves nothing on the GPU that could
+// overlap the next call's use of the shared array.  The wait's own status is
+// ignored (the call already reports the first error).
+struct StaticStreamDrain {
+    cudaStream_t s;
+    bool armed = false;
+    ~StaticStreamDrain() {
+        if (armed) (void)cudaStreamSynchronize(s);
+    }
+};
+
 }  // namespace
 }  // namespace nm
 
@@ -913,6 +933,8 @@ extern "C" int nm_cg_local_static(const nm_csr* A, const double* b, double* x, d
     h.max_iter = max_iter;
     h.guard = 0;
     std::memcpy(hdr, &h, sizeof h);
+    StaticStreamDrain drain{s};
+    drain.armed = true;  // from here on every return waits for `s` first
     NM_CUDA_TRY(cudaMemcpyAsync(d->base, hdr, sizeof hdr, cudaMemcpyHostToDevice, s));
 
     // Ap = A x0 through the fused kernel (its x0.Ax0 by-product is unused;

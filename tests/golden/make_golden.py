@@ -10,7 +10,10 @@ evaluates the reference's accuracy oracle, SciPy (python/verify_accuracy.py:
 small instances.  Outputs:
 
   ref_generators.json  sha256 of (indptr, indices, data) of the reference's
-                       make_laplacian_2d / make_laplacian_3d_fast
+                       make_laplacian_2d / make_laplacian_3d_fast /
+                       make_lattice_gauge / make_random_sparse / make_power_law
+                       (default seeds, and one case each with a caller's
+                       generator and non-default parameters)
   scipy_pins.npz       small reference matrices with x, SciPy y = A @ x, and
                        SciPy CG solutions for b = ones
   c1_probe.json        the 256x256 5-point Laplacian workload: ||A x||_2 for
@@ -49,6 +52,22 @@ def main(ref_root: str) -> None:
         gens[f"laplacian_3d_{L}"] = {
             "indptr": sha(A.indptr.astype(np.int32)), "indices": sha(A.indices.astype(np.int32)),
             "data": sha(A.data.astype(np.float64)), "nnz": int(A.nnz)}
+    def put(key, A):
+        A = A.tocsr()
+        gens[key] = {
+            "indptr": sha(A.indptr.astype(np.int32)), "indices": sha(A.indices.astype(np.int32)),
+            "data": sha(A.data.astype(np.float64)), "nnz": int(A.nnz)}
+
+    for L in (2, 3, 8, 100):
+        put(f"lattice_gauge_{L}", mg.make_lattice_gauge(L))
+    put("lattice_gauge_20_mass0.5_seed3", mg.make_lattice_gauge(20, 0.5, np.random.default_rng(3)))
+    for N in (1, 5, 300, 10000):
+        put(f"random_sparse_{N}", mg.make_random_sparse(N))
+    put("random_sparse_500_nnz4_seed7_nonsym",
+        mg.make_random_sparse(500, 4, np.random.default_rng(7), symmetric=False))
+    for N in (5, 500, 3000):
+        put(f"power_law_{N}", mg.make_power_law(N))
+    put("power_law_800_m5_seed9", mg.make_power_law(800, 5, np.random.default_rng(9)))
     (OUT / "ref_generators.json").write_text(json.dumps(gens, indent=1) + "\n")
 
     pins = {}

@@ -9,11 +9,14 @@ from num_b200 import benchmarks as B
 
 
 def test_registry_sizing_follows_the_reference():
-    # matrix_generators.py:226-230: L = int(N**0.5) / round(N**(1/3))
+    # matrix_generators.py:234-241: L = int(N**0.5) / round(N**(1/3)), N rows otherwise
     assert B.get_matrix("laplacian_2d", 100_000).nrows == 316 * 316
     assert B.get_matrix("laplacian_3d", 1_000_000).nrows == 100 ** 3
-    with pytest.raises(ValueError, match="not available"):
-        B.get_matrix("power_law", 1000)
+    assert B.get_matrix("lattice_gauge", 100_000).nrows == 316 * 316
+    assert B.get_matrix("random_sparse", 3000).nrows == 3000
+    assert B.get_matrix("power_law", 1000).nrows == 1000
+    with pytest.raises(ValueError, match="Unknown matrix"):
+        B.get_matrix("dense", 1000)
 
 
 def test_spmv_metrics_formula():
@@ -49,7 +52,15 @@ def test_cg_scipy_row(tmp_path):
         assert list(csv.DictReader(f))[0]["backend"] == "scipy_cg"
 
 
+@pytest.mark.parametrize("name", ["lattice_gauge", "random_sparse", "power_law"])
+def test_spmv_scipy_rows_on_the_rest_of_the_registry(tmp_path, name):
+    # the reference's own invocation, e.g. benchmark_spmv.py --matrix random_sparse
+    rows = B.run_spmv(["--N", "2500", "--matrix", name, "--backend", "scipy", "--repeat", "3",
+                       "--out", str(tmp_path)])
+    assert rows[0]["backend"] == "scipy_cpu" and rows[0]["nnz"] > rows[0]["N"]
+
+
 def test_cli_usage():
     assert B.main([]) == 2
     with pytest.raises(SystemExit):
-        B.main(["spmv", "--matrix", "lattice_gauge"])
+        B.main(["spmv", "--matrix", "dense"])

@@ -18,10 +18,31 @@ def sha(a):
 REF = json.loads((GOLDEN / "ref_generators.json").read_text())
 
 
+def _build(key):
+    """The generator call a fixture key names (the reference's function of the
+    same name with the same arguments: size, then mass / nnz_per_row / m,
+    then a default_rng seed, then symmetric=False)."""
+    if key.startswith("laplacian_"):
+        kind, L = key.rsplit("_", 1)
+        return (gen.laplacian_2d if kind == "laplacian_2d" else gen.laplacian_3d)(int(L))
+    head, _, rest = key.partition("_")[2].partition("_")
+    name = {"gauge": "lattice_gauge", "sparse": "random_sparse", "law": "power_law"}[head]
+    parts = rest.split("_")
+    size = int(parts[0])
+    if len(parts) == 1:
+        return gen.get_matrix(name, size * size if name == "lattice_gauge" else size)
+    rng = np.random.default_rng(int(parts[2].replace("seed", "")))
+    if name == "lattice_gauge":
+        return gen.lattice_gauge(size, float(parts[1].replace("mass", "")), rng)
+    if name == "random_sparse":
+        return gen.random_sparse(size, int(parts[1].replace("nnz", "")), rng,
+                                 symmetric="nonsym" not in parts)
+    return gen.ba_laplacian(size, int(parts[1].replace("m", "")), rng)
+
+
 @pytest.mark.parametrize("key", sorted(REF))
 def test_matches_reference_generators(key):
-    kind, L = key.rsplit("_", 1)
-    A = (gen.laplacian_2d if kind == "laplacian_2d" else gen.laplacian_3d)(int(L))
+    A = _build(key)
     ref = REF[key]
     assert A.nnz == ref["nnz"]
     assert sha(A.row_ptr) == ref["indptr"]
@@ -77,3 +98,27 @@ def test_spmv_bytes_formula():
     A_nnz, n = 28_518_400, 4_096_000
     assert gen.spmv_bytes(A_nnz, n, n) == 12 * A_nnz + 4 * (n + 1) + 16 * n
     assert abs(gen.spmv_bytes(A_nnz, n, n) / 1e6 - 424.14) < 0.01
+
+
+def test_get_matrix_registry_sizes():
+    # the reference registry's N -> size mapping (python/matrix_generators.py:234-241)
+    assert gen.get_matrix("laplacian_2d", 1000).nrows == 31 * 31
+    assert gen.get_matrix("laplacian_3d", 1000).nrows == 1000
+    assert gen.get_matrix("lattice_gauge", 1000).nrows == 31 * 31
+    assert gen.get_matrix("random_sparse", 1000).nrows == 1000
+    assert gen.get_matrix("power_law", 300).nrows == 300
+    with pytest.raises(ValueError, match="Unknown matrix"):
+        gen.get_matrix("dense", 10)
+
+
+@pytest.mark.parametrize("name", ["lattice_gauge", "random_sparse", "power_law"])
+def test_family_symmetric_sorted(name):
+    A = gen.get_matrix(name, 900)
+    S = A.to_scipy()
+    assert abs(S - S.T).max() == 0
+    for i in range(A.nrows):
+        assert np.all(np.diff(A.col_idx[A.row_ptr[i]:A.row_ptr[i + 1]]) > 0)
+    # diagonally dominant with a positive diagonal (SPD, or PSD for the graph)
+    d = S.diagonal()
+    off = np.asarray(abs(S).sum(axis=1)).ravel() - np.abs(d)
+    assert np.all(d > 0) and np.all(d >= off * (1 - 1e-12))

@@ -80,3 +80,32 @@ def test_static_rejects_more_rows_than_its_scratch(kspmv):
     M, bt, x0 = _problem(kspmv, A, np.ones(A.nrows))
     with pytest.raises(ValueError, match="exceed the fixed scratch"):
         _solve("nm_cg_local_static", M, bt, x0, 1e-8, 10)
+
+
+def test_static_leaves_device_free_memory_unchanged(kspmv):
+    # The contract itself: once the library's CG code is loaded on the device
+    # (one warm-up call), a solve on a matrix it has never seen takes no
+    # device memory -- the free-memory figure is the same before and after.
+    # nm_cg_local on such a matrix would allocate its workspace (about 2 MB
+    # here) and move the figure.
+    lib = _lib.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    A0 = gen.laplacian_2d(64)
+    M0, b0, x0 = _problem(kspmv, A0, np.ones(A0.nrows))
+    r0, _ = _solve("nm_cg_local_static", M0, b0, x0, 1e-8, 1000)
+    assert r0.converged
+    A = gen.laplacian_2d(200)
+    M, bt, _ = _problem(kspmv, A, np.ones(A.nrows))
+    x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
+    res = _lib.CgResult()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        x.zero_()
+        st = lib.nm_cg_local_static(M._h, bt.data_ptr(), x.data_ptr(), 1e-8, 5000,
+                                    C.byref(res), stream)
+        _lib.check(st, "nm_cg_local_static")
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert res.converged
