@@ -88,6 +88,20 @@ int nm_finalize(void);
  * returns NM_ERR_RUNTIME if any kernel gave up since the last call. */
 int nm_check_device_errors(void);
 
+/* Failure-detection hook for tests (no counterpart in the reference, whose
+ * kernels have no bounded waits).  Runs the library's own bounded wait
+ * routine in a kernel where the wait cannot complete -- kind 0: an mbarrier
+ * that expects one arrival more than it gets (one CTA); kind 1: a grid
+ * barrier of `ctas` (1..64) co-resident CTAs that expects one CTA more --
+ * with the wait limited to limit_ms (0 < limit_ms <= 2000) instead of the
+ * library's ~2 s.  Nothing else is pending, so the kernel returns on its own
+ * once the wait gives up.  Synchronises `stream`; *waited_ms (may be NULL)
+ * receives the longest wait.  Returns NM_ERR_RUNTIME when the wait gave up,
+ * as set up, leaving the device error word set for nm_check_device_errors;
+ * NM_OK would mean the wait completed. */
+int nm_test_wait_timeout(int32_t kind, int32_t ctas, double limit_ms, double* waited_ms,
+                         void* stream);
+
 /* ---- CSR matrix ------------------------------------------------------------ */
 
 /* CrsMatrixHandle ctor (src/crs_matrix.hpp:45-72) / upload_csr
@@ -207,9 +221,14 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
 
 /* Process-wide choice of how nm_cg_local / nm_dist_cg_single iterate:
  * 1 (default) one persistent cooperative launch per solve when the device
- * supports it and the matrix's SpMV grid is co-resident; 0 CUDA-graph chunks
- * of three kernels per iteration.  Both give the same iterates, bit for bit.
- * No reference counterpart (an implementation switch). */
+ * supports it and the matrix's SpMV grid is co-resident -- the resident solve
+ * (matrix rows and vectors kept on chip, two grid-wide sums per iteration)
+ * for systems of at most 262,144 rows of at most 8 nonzeros each, else the
+ * persistent TMA-pipelined solve; 2 the persistent TMA-pipelined solve only;
+ * 0 CUDA-graph chunks of three kernels per iteration.  All give the same
+ * iterates, bit for bit (every dot product is summed in one fixed order: per
+ * row block or 256-row tile, then over the blocks).  Other values:
+ * NM_ERR_INVALID.  No reference counterpart (an implementation switch). */
 int nm_cg_set_persistent(int32_t enable);
 
 /* cg_solve_local (src/cg_solver.hpp:133-196; src/bindings.cpp:273-290):
@@ -225,7 +244,7 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * serving engine that reserves nearly all of HBM), and latency-critical loops
  * where cudaMalloc / cudaFree would synchronise the device.  Same algorithm,
  * kernels and result as nm_cg_local, but every scratch vector comes from one
- * fixed device array that is part of the library (about 6.3 MB, held until
+ * fixed device array that is part of the library (about 8.4 MB, held until
  * exit) instead of a per-matrix workspace.  The driver reserves that array
  * on a device when it loads the CG code there: under CUDA's default lazy
  * module loading that is the first call of nm_cg_local_static or nm_cg_local

@@ -57,6 +57,7 @@ _SIGNATURES = {
     "nm_init": ([C.c_int, P_i32, P_i32], C.c_int),
     "nm_finalize": ([], C.c_int),
     "nm_check_device_errors": ([], C.c_int),
+    "nm_test_wait_timeout": ([i32, i32, dbl, C.POINTER(dbl), vp], C.c_int),
     "nm_csr_create": ([vp, vp, vp, C.c_int, i32, i32, C.POINTER(vp)], C.c_int),
     "nm_csr_create_batched": ([i32, vp, vp, vp, vp, vp, C.c_int, C.POINTER(vp)], C.c_int),
     "nm_csr_destroy": ([vp], C.c_int),

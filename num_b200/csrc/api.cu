@@ -130,7 +130,7 @@ extern "C" int nm_check_device_errors(void) {
     }
     if (code & nm::kErrWaitTimeout)
         return fail(NM_ERR_RUNTIME,
-                    "a kernel gave up a bounded wait for its TMA copies; results are invalid");
+                    "a kernel gave up a bounded wait (for TMA copies or a grid barrier); results are invalid");
     if (code) return fail(NM_ERR_RUNTIME, "device error code 0x%x", code);
     return NM_OK;
 }

@@ -65,18 +65,26 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// Row epilogue of K1: store Ap and accumulate p.Ap.
+// Row epilogue of K1: store Ap and accumulate p.Ap; the producer hands one
+// sum per row block to partials[block].
 struct PApEpi {
-    static constexpr bool kBlockSums = false;
+    static constexpr bool kBlockSums = true;
     double* __restrict__ Ap;
     const double* __restrict__ p;
+    double* __restrict__ part;
     double dot;
     __device__ __forceinline__ void operator()(int32_t row, double v) {
         Ap[row] = v;
         dot = fma(__ldg(p + row), v, dot);
     }
-    __device__ __forceinline__ double take() { return 0.0; }
-    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+    __device__ __forceinline__ double take() {
+        const double d = dot;
+        dot = 0.0;
+        return d;
+    }
+    __device__ __forceinline__ void finish_block(int64_t b, const BlockDesc&, double sum) {
+        part[b] = sum;
+    }
 };
 
 template <int TILE, int STAGES>
@@ -86,18 +94,28 @@ __global__ void __launch_bounds__(kCtaThreads)
     if (__ldcg(&st->done)) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES>*>(smem_raw);
-    PApEpi epi{Ap, p, 0.0};
+    __shared__ bool am_last;
+    PApEpi epi{Ap, p, partials, 0.0};
     const bool ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
     if (!ok && threadIdx.x == 0) {
-        // A bounded wait gave up: end the solve; every CTA still takes part in
-        // the reduction below so the arrival counter stays consistent.
+        // A bounded wait gave up: end the solve; every CTA still arrives below
+        // so the arrival counter stays consistent.
         atomicExch(&st->status, kCgDeviceError);
         atomicExch(&st->done, 1);
     }
-    double part[1] = {block_sum(epi.dot, sm.red)};
-    double tot[1];
-    if (grid_reduce_last<1>(part, partials, &st->counter, tot, sm.red)) {
-        const double pAp = tot[0];
+    // the last CTA to arrive adds the per-block sums in the fixed order
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        am_last = atomicAdd(&st->counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    const double pAp_t = reduce256(partials, M.nblk, sm.red);
+    if (threadIdx.x == 0) {
+        st->counter = 0u;
+        const double pAp = pAp_t;
         st->pAp = pAp;
         if (st->guard && fabs(pAp) < 1e-300) {
             st->status = kCgBreakdown;
@@ -178,82 +196,36 @@ __global__ void __launch_bounds__(kThreads)
 // others give up at their next barrier.
 // ---------------------------------------------------------------------------
 
-// Grid barrier on (count, gen); returns false when the wait gave up or a CTA
-// has marked the solve failed (*status == kCgDeviceError) -- read once, by
-// thread 0, so every thread of the CTA gets the same answer.
-__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen,
-                                             unsigned int* err, const int32_t* status,
-                                             bool* flag) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        bool ok = true;
-        // Arrival is an acq_rel add on count (a release sequence: the last
-        // arriver acquires every CTA's writes); it resets count and releases
-        // gen, on which the others spin with acquire loads.
-        unsigned int g0, prev;
-        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(g0) : "l"(gen) : "memory");
-        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
-                     : "=r"(prev) : "l"(count) : "memory");
-        if (prev == gridDim.x - 1) {
-            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(count) : "memory");
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(gen) : "memory");
-        } else {
-            const uint64_t t0 = global_timer_ns();
-            for (uint32_t it = 0;; ++it) {
-                unsigned int g;
-                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(gen) : "memory");
-                if (g != g0) break;
-                if ((it & 255u) == 0 && (global_timer_ns() - t0 > kWaitLimitNs || it > (1u << 30))) {
-                    atomicOr(err, kErrWaitTimeout);
-                    ok = false;
-                    break;
-                }
-            }
-        }
-        *flag = ok && __ldcg(status) != kCgDeviceError;
-    }
-    __syncthreads();
-    return *flag;
-}
-
-// Sum over the first 8 warps (the 256 threads of a cg_update_xr_kernel CTA);
-// valid in thread 0.  All threads of the CTA call it.
-__device__ __forceinline__ double block_sum8(double v, double* scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_sum(v);
-    if (lane == 0 && warp < kWarps) scratch[warp] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) s += scratch[w];
-    }
-    __syncthreads();
-    return s;
-}
-
 struct CoopPApEpi {
-    static constexpr bool kBlockSums = false;
+    static constexpr bool kBlockSums = true;
     double* __restrict__ Ap;
     const double* __restrict__ p;
+    double* __restrict__ part;  // p.Ap per row block
     double dot;
     __device__ __forceinline__ void operator()(int32_t row, double v) {
         Ap[row] = v;
         dot = fma(__ldcg(p + row), v, dot);
     }
-    __device__ __forceinline__ double take() { return 0.0; }
-    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+    __device__ __forceinline__ double take() {
+        const double d = dot;
+        dot = 0.0;
+        return d;
+    }
+    __device__ __forceinline__ void finish_block(int64_t b, const BlockDesc&, double sum) {
+        part[b] = sum;
+    }
 };
 
 // Row epilogue of the two-barrier form: the row's new direction
 // p'[row] = fma(beta, p[row], r[row]) (what the three-kernel path's p update
 // computes) goes to the other p buffer, then Ap and p'.Ap as in CoopPApEpi.
 struct CoopFormPApEpi {
-    static constexpr bool kBlockSums = false;
+    static constexpr bool kBlockSums = true;
     double* __restrict__ Ap;
     const double* __restrict__ p;
     const double* __restrict__ r;
     double* __restrict__ pn;
+    double* __restrict__ part;
     double beta;
     double dot;
     __device__ __forceinline__ void operator()(int32_t row, double v) {
@@ -262,8 +234,14 @@ struct CoopFormPApEpi {
         pn[row] = pr;
         dot = fma(pr, v, dot);
     }
-    __device__ __forceinline__ double take() { return 0.0; }
-    __device__ __forceinline__ void finish_block(int64_t, const BlockDesc&, double) {}
+    __device__ __forceinline__ double take() {
+        const double d = dot;
+        dot = 0.0;
+        return d;
+    }
+    __device__ __forceinline__ void finish_block(int64_t b, const BlockDesc&, double sum) {
+        part[b] = sum;
+    }
 };
 
 // FORMED: the two-barrier form.  Phase C disappears: the next iteration's
@@ -296,18 +274,15 @@ __global__ void __launch_bounds__(kCtaThreads)
         // ---- A: Ap = A p, p.Ap (FORMED: p' = fma(beta_prev, p, r) formed on the fly) ----
         double* pa_vec = p;  // the direction of this iteration
         bool ok;
-        double dot;
         if constexpr (FORMED) {
             pa_vec = p2;
-            CoopFormPApEpi epi{Ap, p, r, p2, beta_prev, 0.0};
+            CoopFormPApEpi epi{Ap, p, r, p2, part_a, beta_prev, 0.0};
             ok = spmv_pipeline<double, double, double, TILE, STAGES, true>(M, p, sm, epi, err,
                                                                           AllBlocks(), r,
                                                                           beta_prev);
-            dot = epi.dot;
         } else {
-            CoopPApEpi epi{Ap, p, 0.0};
+            CoopPApEpi epi{Ap, p, part_a, 0.0};
             ok = spmv_pipeline<double, double, double, TILE, STAGES>(M, p, sm, epi, err);
-            dot = epi.dot;
         }
         __syncthreads();
         if (t == 0) {  // the ring's barriers are initialised again by the next SpMV
@@ -320,12 +295,9 @@ __global__ void __launch_bounds__(kCtaThreads)
             }
         }
         if (!ok) atomicExch(&st->status, kCgDeviceError);
-        const double pa = block_sum(dot, sm.red);
-        if (t == 0) part_a[blockIdx.x] = pa;
+        // the producer left one p.Ap sum per row block in part_a
         if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
-        double s = 0.0;
-        for (unsigned i = t; i < gridDim.x; i += blockDim.x) s += __ldcg(part_a + i);
-        const double pAp = block_sum(s, sm.red);
+        const double pAp = reduce256(part_a, M.nblk, sm.red);
         if (t == 0) bcast[0] = pAp;
         __syncthreads();
         const double pAp_all = bcast[0];
@@ -357,10 +329,7 @@ __global__ void __launch_bounds__(kCtaThreads)
             if (t == 0) part_b[v] = pv;
         }
         if (!grid_barrier(&st->bar_count, &st->bar_gen, err, &st->status, &flag)) { failed = true; break; }
-        double s2 = 0.0;
-        if (t < kThreads)
-            for (int i = t; i < grid_vec; i += kThreads) s2 += __ldcg(part_b + i);
-        const double rr_new0 = block_sum8(s2, sm.red);
+        const double rr_new0 = reduce256(part_b, grid_vec, sm.red);
         if (t == 0) bcast[1] = rr_new0;
         __syncthreads();
         const double rr_new = bcast[1];
@@ -452,6 +421,7 @@ CgWorkspace::~CgWorkspace() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     cudaFree(dmem);
+    if (res_mem) cudaFree(res_mem);
     pinned_slots().put(h_in);
     pinned_slots().put(h_out);
 }
@@ -518,7 +488,10 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     }
     if (st != NM_OK) return st;
     ws->grid_spmv = spmv_grid(A, occ);
-    ws->partials_cap = 2 * std::max(ws->grid_spmv, ws->grid_vec);
+    // K1 leaves one sum per row block, K2 one per vector CTA, the initial
+    // kernel two per vector CTA; the persistent solve keeps the block sums and
+    // the vector sums side by side
+    ws->partials_cap = static_cast<int>(A->nblk) + 2 * ws->grid_vec;
     {
         // r, p, Ap, p2, the CTA partial sums and the state in one allocation
         // (each part 256-byte aligned)
@@ -550,6 +523,10 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
         ws->coop = coop_ok && int64_t(occ_c) * sm_count() >= ws->grid_spmv &&
                    n <= kCoopMaxRows;
         ws->coop_formed = ws->coop && int64_t(occ_f) * sm_count() >= ws->grid_spmv;
+        if (coop_ok) {
+            st = plan_resident(A, ws.get());
+            if (st != NM_OK) return st;
+        }
     }
     ws->err = device_error_word();
     if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
@@ -615,7 +592,7 @@ int launch_coop_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
     CsrView<double> M = A->view<double>();
     M.stage_x = 1;  // p, p2 and r are workspace vectors (256-byte aligned)
     double* part_a = ws->partials;
-    double* part_b = ws->partials + ws->grid_spmv;
+    double* part_b = ws->partials + A->nblk;
     int grid_vec = ws->grid_vec;
     int64_t n = ws->n;
     void* args[] = {&M,     &ws->st, &ws->p,    &ws->p2, &ws->Ap, &ws->r,
@@ -675,10 +652,12 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
                                                      ws->partials);
     NM_CHECK_LAUNCH();
 
-    const bool coop = ws->coop && g_cg_persistent.load();
+    const int mode = g_cg_persistent.load();
+    const bool resident = ws->resident && mode == 1;
+    const bool coop = resident || (ws->coop && mode >= 1);
     if (coop) {
         // the whole iteration loop in one persistent launch
-        st = launch_coop(A, ws, s);
+        st = resident ? launch_resident(A, ws, s) : launch_coop(A, ws, s);
         if (st != NM_OK) return st;
         NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         NM_CUDA_TRY(cudaStreamSynchronize(s));
@@ -712,7 +691,9 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
 
 extern "C" int nm_cg_set_persistent(int32_t enable) {
     nm::clear_error();
-    nm::g_cg_persistent.store(enable ? 1 : 0);
+    if (enable < 0 || enable > 2)
+        return nm::fail(NM_ERR_INVALID, "nm_cg_set_persistent: 0, 1 or 2");
+    nm::g_cg_persistent.store(enable);
     return NM_OK;
 }
 
@@ -734,7 +715,7 @@ extern "C" int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, in
 // device and stall every other stream.  nm_cg_local caches a workspace per
 // matrix, allocated on first use; this variant instead takes r, p, Ap, the
 // CTA partial sums, the device-resident CG state and the error word from one
-// file-scope device array that is part of the loaded library (about 6.3 MB,
+// file-scope device array that is part of the loaded library (about 8.4 MB,
 // held until the process exits by every GPU on which this file's module has
 // been loaded).  Under CUDA's default lazy module loading the driver loads the
 // module, and so reserves the array, on the first use of this file's kernels
@@ -758,7 +739,9 @@ namespace nm {
 namespace {
 
 constexpr int64_t kStaticCgMaxRows = 262144;
-constexpr int kStaticCgMaxPartials = 4096;
+// one p.Ap sum per row block (at most one block per row) or two sums per
+// vector CTA, whichever is more
+constexpr int kStaticCgMaxPartials = static_cast<int>(kStaticCgMaxRows) + 4096;
 constexpr size_t kStaticErrOff = 512;      // error word, after the CgState
 constexpr size_t kStaticPartOff = 1024;    // CTA partial sums
 constexpr size_t kStaticVecOff = kStaticPartOff + sizeof(double) * kStaticCgMaxPartials;
@@ -912,9 +895,9 @@ extern "C" int nm_cg_local_static(const nm_csr* A, const double* b, double* x, d
     L.grid_spmv = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(int64_t(d->sms) * mult, A->nblk)));
     L.grid_vec = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>((L.n + kThreads - 1) / kThreads, int64_t(d->sms) * 8)));
-    if (2 * std::max(L.grid_spmv, L.grid_vec) > kStaticCgMaxPartials)
-        return fail(NM_ERR_INVALID, "nm_cg_local_static: grid of %d CTAs exceeds the scratch",
-                    std::max(L.grid_spmv, L.grid_vec));
+    if (std::max<int64_t>(A->nblk, 2 * int64_t(L.grid_vec)) > kStaticCgMaxPartials)
+        return fail(NM_ERR_INVALID, "nm_cg_local_static: %d row blocks exceed the scratch",
+                    A->nblk);
     L.st = reinterpret_cast<CgState*>(d->base);
     L.err = reinterpret_cast<unsigned int*>(d->base + kStaticErrOff);
     L.partials = reinterpret_cast<double*>(d->base + kStaticPartOff);

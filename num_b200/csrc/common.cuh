@@ -173,16 +173,23 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 
 // Wait for phase `parity` of `bar` to complete, giving up after ~2 s of
 // wall time (and after a fixed number of polls) so that no fault can turn
-// into a hang.  Returns false when it gave up.
+// into a hang.  Returns false when it gave up.  `limit_ns` is lowered only by
+// the failure-detection test kernels (nm_test_wait_timeout).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t it = 0; it < (1u << 30); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) return false;
+        if ((it & 255u) == 0 && global_timer_ns() - t0 > limit_ns) return false;
     }
     return false;
+}
+
+// Plain arrival (no transaction bytes) on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 template <typename T>

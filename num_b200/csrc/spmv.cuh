@@ -72,10 +72,6 @@ __device__ __forceinline__ bool consumer_sync_or(bool pred) {
     return r != 0;
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Deterministic sum over the consumer threads; valid in consumer thread 0.
 template <typename T>
 __device__ __forceinline__ T consumer_sum(T v, T* scratch) {

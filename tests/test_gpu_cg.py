@@ -264,12 +264,16 @@ def _arrow_spd(n, rng):
     return gen.Csr(rp, ci, v, n, n)
 
 
-# The persistent solve runs in its two-barrier form (direction formed inside
-# the SpMV) while the SpMV grid fits it -- the 256^2 and 40^3 Laplacians, the
-# 30,000-row banded system (scattered off-band columns: the gather path) and
-# the arrow matrix (a long row) -- and in its three-barrier form for the
-# 64^3 Laplacian and the 48^3 variable-coefficient system (grids of 444 and
-# 432 CTAs); the 300,000-row banded system takes the graph path both ways.
+# Mode 1 runs the resident solve where it applies (the 256^2 and 40^3
+# Laplacians and the 48^3 variable-coefficient system: rows of <= 8 nonzeros,
+# whole 256-row tiles) and the TMA-pipelined persistent solve elsewhere; mode 2
+# forces the latter, which runs in its two-barrier form (direction formed
+# inside the SpMV) while the SpMV grid fits it -- the 256^2 and 40^3
+# Laplacians, the 30,000-row banded system (scattered off-band columns: the
+# gather path) and the arrow matrix (a long row) -- and in its three-barrier
+# form for the 64^3 Laplacian and the 48^3 variable-coefficient system (grids
+# of 444 and 432 CTAs); mode 0 is the CUDA-graph path; the 300,000-row banded
+# system takes the graph path in every mode.
 @pytest.mark.parametrize("case", ["lap2d_256", "lap3d_40", "banded_30k", "arrow_20k",
                                   "lap3d_64", "varcoef_48", "banded"])
 def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
@@ -294,7 +298,7 @@ def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
     out = []
     try:
-        for persistent in (1, 0, 1):
+        for persistent in (1, 0, 2, 1):
             nmlib.nm_cg_set_persistent(persistent)
             x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
             info = kspmv.cg_solve_local(M, b, x, tol=1e-9, max_iter=3000)
