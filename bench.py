@@ -836,57 +836,82 @@ def run_engine(args, rank, world, local_rank):
 
 # ---- our arm: served request stream (C5) -----------------------------------------------
 
-def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, local_rank=0):
-    """Served runs of the stream on one solver, and the plain drop-in once."""
+def served_bytes(requests, rec, precision):
+    """Algorithmic bytes of the engine iterations a served pass ran: per
+    request its inner iterations times engine_iter_bytes and its refinement
+    steps times engine_outer_bytes."""
+    vb = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
+    tb = 8 if precision == "fp64" else 4
+    tot = 0
+    for (_, A, _, _), r in zip(requests, rec):
+        tot += r["iters"] * engine_iter_bytes(A.nnz, A.nrows, vb, tb)
+        tot += r.get("outer", 0) * engine_outer_bytes(A.nnz, A.nrows, tb)
+    return tot
+
+
+def serve_measure(dev, requests, runs, warmup, arena_bytes, with_plain=True, local_rank=0,
+                  precision="fp32", precond="jacobi", check_limit=None, plain_passes=2):
+    """Served runs of the stream on one solver, and the plain drop-in.
+
+    Streams longer than check_limit requests (None: no limit) check the true
+    FP64 residual, and compare with the plain drop-in's solution, on their
+    first check_limit requests only, and warm up on those too (all arriving
+    at once) instead of on whole passes."""
     import torch
 
     from num_b200 import serve
     from num_b200.solver import BatchSolver, arena_for
-    rows, nnz = arena_for(arena_bytes, nnz_per_row=5.0, precision="fp32")
-    S = BatchSolver(rows, nnz, 1024, precision="fp32")
+    rows, nnz = arena_for(arena_bytes, nnz_per_row=5.0, precision=precision)
+    S = BatchSolver(rows, nnz, 1024, precision=precision, precond=precond)
     ext = torch.cuda.ExternalStream(S.stream(), device=dev)
+    head = requests if check_limit is None or len(requests) <= check_limit else \
+        [(0.0, A, b, k) for (_, A, b, k) in requests[:check_limit]]
     errs = []
     sols = {}
 
     def check_fn(i, x, info):
-        _, A, b, _ = requests[i]
+        _, A, b, _ = head[i]
         errs.append(float(np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)))
         sols[i] = np.array(x, copy=True)
 
     # untimed: one pass that checks every result's true FP64 residual, and the
     # warm-up passes
-    serve.serve(requests, S, tol=1e-8, chunk=16, check=check_fn)
+    serve.serve(head, S, tol=1e-8, chunk=16, check=check_fn)
     for _ in range(max(0, warmup - 1)):
-        serve.serve(requests, S, tol=1e-8, chunk=16)
-    stats = []
+        serve.serve(head, S, tol=1e-8, chunk=16)
+    stats, recs = [], []
     c0 = S.counters()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clk = ClockSampler(local_rank)
     with clk:
         t0.record(ext)
         for k in range(runs):
-            st, _ = serve.serve(requests, S, tol=1e-8, chunk=16)
+            st, rec = serve.serve(requests, S, tol=1e-8, chunk=16)
             stats.append(st)
+            recs.append(rec)
         t1.record(ext)
         torch.cuda.synchronize(dev)
     c1 = S.counters()
+    alg = sum(served_bytes(requests, rec, precision) for rec in recs)
     out = {"ms": t0.elapsed_time(t1), "stats": stats, "ctr0": c0, "ctr1": c1,
-           "max_true_residual": max(errs) if errs else None, "clocks": clk.summary()}
+           "algorithmic_bytes": alg, "max_true_residual": max(errs) if errs else None,
+           "checked": len(head), "clocks": clk.summary()}
+    del S
     if with_plain:
         # the plain drop-in's pass time varies with host work (uploads, frees):
-        # compare against the better of two passes
-        runs = [serve.serve_plain(requests, tol=1e-8)[0] for _ in range(2)]
-        pst = max(runs, key=lambda r: r["solves_per_s"])
-        pst["passes_solves_per_s"] = [round(r["solves_per_s"], 3) for r in runs]
+        # compare against the better of the passes
+        runs_p = [serve.serve_plain(requests, tol=1e-8)[0] for _ in range(plain_passes)]
+        pst = max(runs_p, key=lambda r: r["solves_per_s"])
+        pst["passes_solves_per_s"] = [round(r["solves_per_s"], 3) for r in runs_p]
         out["plain"] = pst
-        # untimed: every served (FP32 + refinement) result against the plain
-        # FP64 drop-in's solution of the same request
+        # untimed: the served results of the checked requests against the
+        # plain FP64 drop-in's solutions of the same requests
         rel = []
 
         def cmp_fn(i, x, info):
             if i in sols:
                 rel.append(float(np.linalg.norm(sols[i] - x) / max(np.linalg.norm(x), 1e-300)))
-        serve.serve_plain(requests, tol=1e-8, check=cmp_fn)
+        serve.serve_plain(head, tol=1e-8, check=cmp_fn)
         out["max_rel_error_vs_fp64"] = max(rel) if rel else None
     return out
 
@@ -896,11 +921,15 @@ def run_serve(args, rank, world, local_rank):
 
     from num_b200 import serve
     dev = torch.device("cuda", local_rank)
-    desc, _, precision = WORKLOADS[args.workload]
-    requests = serve.make_requests(args.requests, rate=args.rate, seed=4)
+    desc, _, _ = WORKLOADS[args.workload]
+    precision = args.serve_precision
+    requests = serve.make_requests(args.requests, rate=args.rate, seed=4, pool=args.pool)
+    big = len(requests) > 1000
     barrier(world)
     r = serve_measure(dev, requests, args.steps, args.warmup, args.arena_gb * 1e9,
-                      local_rank=local_rank)
+                      local_rank=local_rank, precision=precision, precond=args.serve_precond,
+                      check_limit=300 if big else None, plain_passes=1 if big else 2,
+                      with_plain=not args.no_plain)
     barrier(world)
     ms = max_over_ranks([r["ms"]], world, dev)[0]
     if rank != 0:
@@ -911,34 +940,41 @@ def run_serve(args, rank, world, local_rank):
     c0, c1 = r["ctr0"], r["ctr1"]
     p50 = statistics.median(s["p50_ms"] for s in r["stats"])
     p99 = statistics.median(s["p99_ms"] for s in r["stats"])
-    plain = r["plain"]
     tot_rows = sum(q[1].nrows for q in requests)
     tot_nnz = sum(q[1].nnz for q in requests)
+    inner = {"fp32": "fp32 values + vectors, FP64 refinement",
+             "bf16": "bf16 values, fp32 vectors, FP64 refinement",
+             "fp64": "fp64 values + vectors, no refinement"}[precision]
     config = {"workload": desc, "name": args.workload, "requests": n,
               "arrival_rate_per_s": args.rate if args.rate > 0 else "all at t=0 (saturated)",
+              "distinct_systems": min(n, args.pool) if args.pool else n,
               "rows_total": tot_rows, "nnz_total": tot_nnz, "tol": 1e-8,
-              "arena_gb_cap": args.arena_gb, "inner": "fp32 values + vectors, FP64 refinement",
+              "arena_gb_cap": args.arena_gb, "inner": inner,
+              "preconditioner": args.serve_precond,
               "max_true_residual_fp64": r["max_true_residual"],
+              "checked_requests": r["checked"],
               "max_rel_error_vs_fp64_dropin": r.get("max_rel_error_vs_fp64"),
               "parallelism": f"replicas x{world}",
               "api": "num_b200.serve.serve over BatchSolver (nm_solver_* C ABI)"}
+    if big:
+        config["note"] = ("requests i >= pool reuse system i mod pool (an i.i.d. sample of "
+                          "the distribution); every request has its own Poisson arrival; "
+                          "residual / error checks and warm-up on the first 300 requests")
     line = base_line(args, world, round(world * solves_s, 3), "solves/s", ms_per, precision,
                      config)
     peak, peak_src = measured_peak()
     dev_s = (c1["s_device"] - c0["s_device"]) / args.steps
+    achieved = r["algorithmic_bytes"] / args.steps / dev_s / 1e9 if dev_s > 0 else None
     line.update({
         "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3)},
-        "plain_fp64_drop_in": {"solves_per_s": round(plain["solves_per_s"], 3),
-                               "p50_ms": round(plain["p50_ms"], 3),
-                               "p99_ms": round(plain["p99_ms"], 3),
-                               "passes": plain["passes_solves_per_s"],
-                               "note": "the better of two passes",
-                               "api": "kokkos_spmv.upload_csr + cg_solve_local, one request at "
-                                      "a time in arrival order"},
-        "ratio_vs_plain": round(solves_s / plain["solves_per_s"], 3),
-        "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s",
-                     "frac": None, "peak_source": peak_src, "traffic": None,
-                     "kernel": "served engine steps",
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None,
+                     "peak_source": peak_src, "traffic": None,
+                     "kernel": "served engine steps: summed algorithmic bytes of every "
+                               "request's inner iterations and refinement steps over the "
+                               "steps' device time",
+                     "device_busy_s_per_pass": round(dev_s, 4),
                      "device_busy_frac": round(dev_s / (ms_per * 1e-3), 4)},
         "e2e": {"value": round(world * solves_s, 3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(tot_nnz * 16 + tot_rows * 12),
@@ -949,6 +985,15 @@ def run_serve(args, rank, world, local_rank):
                             (c1["outer_launches"] - c0["outer_launches"]) * 6),
         "clocks": r["clocks"],
     })
+    if "plain" in r:
+        plain = r["plain"]
+        line["plain_fp64_drop_in"] = {
+            "solves_per_s": round(plain["solves_per_s"], 3), "p50_ms": round(plain["p50_ms"], 3),
+            "p99_ms": round(plain["p99_ms"], 3), "passes": plain["passes_solves_per_s"],
+            "note": "the better of the passes",
+            "api": "kokkos_spmv.upload_csr + cg_solve_local, one request at a time in "
+                   "arrival order"}
+        line["ratio_vs_plain"] = round(solves_s / plain["solves_per_s"], 3)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_serve(requests, budget_s=args.cpu_seconds)
     return line
@@ -1193,7 +1238,7 @@ def run_reference(args, rank, world):
         ms_step = 1e3 / val
     else:  # serve
         from num_b200 import serve
-        requests = serve.make_requests(args.requests, rate=args.rate, seed=4)
+        requests = serve.make_requests(args.requests, rate=args.rate, seed=4, pool=args.pool)
         cb = cpu_baseline_serve(requests, budget_s=60.0)
         val, unit, sample = cb["value"], "solves/s", cb["sample"] + f" ({note})"
         cfg = {"workload": desc, "name": args.workload, "requests": len(requests)}
@@ -1234,6 +1279,14 @@ def main():
     ap.add_argument("--rate", type=float, default=0.0,
                     help="serve_c5: Poisson arrival rate (req/s); 0 = all at t=0")
     ap.add_argument("--arena-gb", type=float, default=64.0, help="serve_c5: arena cap")
+    ap.add_argument("--pool", type=int, default=1000,
+                    help="serve_c5: distinct systems; longer streams reuse them")
+    ap.add_argument("--serve-precision", default="fp32", choices=["fp32", "bf16", "fp64"],
+                    help="serve_c5: the engine's inner precision")
+    ap.add_argument("--serve-precond", default="jacobi", choices=["jacobi", "none"],
+                    help="serve_c5: the engine's preconditioner")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="serve_c5: skip the plain FP64 drop-in comparison")
     args = ap.parse_args()
     kind = WORKLOADS[args.workload][1]
     if args.steps <= 0:

@@ -222,6 +222,10 @@ int rebuild_blocks(nm_csr* A) {
         A->warp_gather = A->tune.kernel == NM_KERNEL_GATHER ||
                          (A->tune.kernel == NM_KERNEL_AUTO && scattered);
     }
+    if (A->warp_gather && !A->sell_tried) {
+        const int st = build_sell(A);
+        if (st != NM_OK) return st;
+    }
     if (A->d_blk) {
         cudaFree(A->d_blk);
         A->d_blk = nullptr;
@@ -280,6 +284,11 @@ nm_csr::~nm_csr() {
     if (d_values) cudaFree(d_values);
     if (d_blk) cudaFree(d_blk);
     if (d_desc) cudaFree(d_desc);
+    if (d_sell_ptr) cudaFree(d_sell_ptr);
+    if (d_sell_row) cudaFree(d_sell_row);
+    if (d_sell_len) cudaFree(d_sell_len);
+    if (d_sell_col) cudaFree(d_sell_col);
+    if (d_sell_val) cudaFree(d_sell_val);
 }
 
 using nm::fail;

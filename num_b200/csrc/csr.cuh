@@ -94,6 +94,21 @@ struct nm_csr {
     // from tune.kernel (AUTO: most nonzeros in blocks without x windows and no
     // row longer than kWarpGatherMaxRow).
     bool warp_gather = false;
+    // The gather kernel's copy of the matrix (built the first time that kernel
+    // is selected, kept until the handle is freed): rows sorted by length
+    // (descending, stable) within windows of kSellWindow rows, cut into slices
+    // of 32 sorted rows, each slice stored column-major -- entry k of the
+    // slice's lane l at sell_ptr[s] + 32 k + l, zero-padded to the slice's
+    // longest row -- with the original row and the length of every sorted
+    // position.  A matrix whose padding would exceed its nonzeros keeps the
+    // per-group gather kernel instead (sell_ready false).
+    bool sell_tried = false, sell_ready = false;
+    int32_t sell_slices = 0;
+    int64_t* d_sell_ptr = nullptr;
+    int32_t* d_sell_row = nullptr;
+    int32_t* d_sell_len = nullptr;
+    int32_t* d_sell_col = nullptr;
+    void* d_sell_val = nullptr;
     std::vector<int32_t> h_row_ptr;  // kept to rebuild the partition on retuning
     std::vector<int32_t> h_col_idx;  // kept to rebuild the x windows on retuning
     // Many-matrix handles: per-matrix row / column offsets (count + 1 each).
@@ -126,6 +141,11 @@ size_t spmv_smem_for(int dtype, int tile, int stages);
 int rebuild_blocks(nm_csr* A);
 // Longest row the warp-gather kernel takes (each row is summed by one lane).
 constexpr int32_t kWarpGatherMaxRow = 4096;
+// Rows sorted by length together in the gather kernel's sliced copy.
+constexpr int32_t kSellWindow = 1024;
+// Builds A's sliced copy for the gather kernel once (spmv.cu); NM_OK also
+// when the layout would pad too much (A->sell_ready stays false).
+int build_sell(nm_csr* A);
 // Drops A's cached CG workspace (its graphs hold the current descriptors).
 void reset_cg(nm_csr* A);
 // Nonzeros of the Laplacian on an L^dim grid (dim 2: 5-point, dim 3: 7-point).

@@ -1,7 +1,9 @@
 // spmv.cu -- plain SpMV and multi-RHS SpMV kernels and their launchers.
 #include "spmv.cuh"
 
+#include <algorithm>
 #include <atomic>
+#include <vector>
 
 namespace nm {
 
@@ -125,6 +127,188 @@ static int launch_gather(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     return NM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Sliced gather kernel: the same serial CSR-order row sums, from the
+// length-sorted sliced copy (nm_csr::d_sell_*).  One warp per slice of 32
+// sorted rows, slices strided over the resident warps; lane l owns the
+// slice's row l and adds its products in its own register, reading entry k of
+// all 32 rows with one coalesced load per array (the slice is column-major)
+// and gathering x[col] through L2, kSellU entries ahead.  The 32 rows of a
+// slice have nearly the same length (sorted within kSellWindow rows), so no
+// lane waits long for the others, and no product goes through shared memory
+// -- the x gathers are left as the only scattered traffic.  Slice metadata is
+// fetched one slice ahead.
+constexpr int kSellThreads = 128;
+constexpr int kSellU = 8;
+
+template <typename V, typename X, typename A>
+__global__ void __launch_bounds__(kSellThreads)
+    spmv_sell_kernel(const int64_t* __restrict__ sp, const int32_t* __restrict__ srow,
+                     const int32_t* __restrict__ slen, const int32_t* __restrict__ col,
+                     const V* __restrict__ val, const X* __restrict__ x, X* __restrict__ y,
+                     int32_t nslices, int32_t nrows) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = int64_t(gridDim.x) * (kSellThreads / 32);
+    int64_t s = (int64_t(blockIdx.x) * kSellThreads + threadIdx.x) >> 5;  // same for the warp
+    auto meta = [&](int64_t ss, int64_t& b, int64_t& e, int32_t& r, int32_t& len) {
+        b = e = 0;
+        r = -1;
+        len = 0;
+        if (ss < nslices) {
+            b = __ldg(sp + ss);
+            e = __ldg(sp + ss + 1);
+            const int64_t i = ss * 32 + lane;
+            if (i < nrows) {
+                r = __ldg(srow + i);
+                len = __ldg(slen + i);
+            }
+        }
+    };
+    int64_t nb, ne;
+    int32_t nr, nl;
+    meta(s, nb, ne, nr, nl);
+    for (; s < nslices; s += nw) {
+        const int64_t base = nb;
+        const int32_t width = static_cast<int32_t>((ne - nb) >> 5);
+        const int32_t r = nr, len = nl;
+        meta(s + nw, nb, ne, nr, nl);
+        const int32_t* __restrict__ cp = col + base + lane;
+        const V* __restrict__ vp = val + base + lane;
+        A acc = A(0);
+        int32_t k = 0;
+        for (; k + kSellU <= width; k += kSellU) {
+            int32_t c[kSellU];
+            V v[kSellU];
+            X xv[kSellU];
+#pragma unroll
+            for (int u = 0; u < kSellU; ++u) {
+                c[u] = __ldcs(cp + int64_t(k + u) * 32);
+                v[u] = ld_value_cs(vp + int64_t(k + u) * 32);
+            }
+#pragma unroll
+            for (int u = 0; u < kSellU; ++u) xv[u] = k + u < len ? __ldcg(x + c[u]) : X(0);
+#pragma unroll
+            for (int u = 0; u < kSellU; ++u)
+                if (k + u < len) acc = add_rn(acc, mul_rn(widen<V, A>(v[u]), static_cast<A>(xv[u])));
+        }
+        for (; k < width; ++k) {
+            if (k < len) {
+                const int32_t c = __ldcs(cp + int64_t(k) * 32);
+                const V v = ld_value_cs(vp + int64_t(k) * 32);
+                acc = add_rn(acc, mul_rn(widen<V, A>(v), static_cast<A>(__ldcg(x + c))));
+            }
+        }
+        if (r >= 0) y[r] = static_cast<X>(acc);
+    }
+}
+
+// Fills the sliced copy from the device CSR: one warp per slice, lane l
+// copies the row of sorted position 32 s + l and zero-pads it to the slice
+// width.
+template <typename V>
+__global__ void sell_fill_kernel(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 const V* __restrict__ vals, const int64_t* __restrict__ sp,
+                                 const int32_t* __restrict__ srow, const int32_t* __restrict__ slen,
+                                 int32_t* __restrict__ col, V* __restrict__ val, int32_t nslices,
+                                 int32_t nrows) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = int64_t(gridDim.x) * (blockDim.x / 32);
+    for (int64_t s = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; s < nslices; s += nw) {
+        const int64_t base = sp[s];
+        const int32_t width = static_cast<int32_t>((sp[s + 1] - base) >> 5);
+        const int64_t i = s * 32 + lane;
+        int32_t z0 = 0, len = 0;
+        if (i < nrows) {
+            z0 = rp[srow[i]];
+            len = slen[i];
+        }
+        for (int32_t k = 0; k < width; ++k) {
+            const int64_t dst = base + int64_t(k) * 32 + lane;
+            col[dst] = k < len ? ci[z0 + k] : 0;
+            val[dst] = k < len ? vals[z0 + k] : V(0.0f);
+        }
+    }
+}
+
+template <typename V>
+static int fill_sell(nm_csr* A, int64_t total) {
+    NM_CUDA_TRY(cudaMalloc(&A->d_sell_col, sizeof(int32_t) * size_t(total)));
+    NM_CUDA_TRY(cudaMalloc(&A->d_sell_val, sizeof(V) * size_t(total)));
+    const int64_t blocks = std::min<int64_t>((int64_t(A->sell_slices) + 7) / 8, 65535);
+    sell_fill_kernel<V><<<static_cast<int>(std::max<int64_t>(1, blocks)), 256>>>(
+        A->d_row_ptr, A->d_col_idx, static_cast<const V*>(A->d_values), A->d_sell_ptr,
+        A->d_sell_row, A->d_sell_len, A->d_sell_col, static_cast<V*>(A->d_sell_val),
+        A->sell_slices, A->nrows);
+    NM_CHECK_LAUNCH();
+    NM_CUDA_TRY(cudaDeviceSynchronize());
+    return NM_OK;
+}
+
+template <typename V, typename X, typename A>
+static int launch_sell(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+    static std::atomic<int> occ_cache{0};  // resident CTAs per SM (same on every device here)
+    int occ = occ_cache.load(std::memory_order_relaxed);
+    if (occ == 0) {
+        NM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, spmv_sell_kernel<V, X, A>, kSellThreads, 0));
+        occ = occ > 0 ? occ : 1;
+        occ_cache.store(occ, std::memory_order_relaxed);
+    }
+    const int64_t need = (int64_t(Am->sell_slices) + kSellThreads / 32 - 1) / (kSellThreads / 32);
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sm_count()) * occ)));
+    spmv_sell_kernel<V, X, A><<<grid, kSellThreads, 0, s>>>(
+        Am->d_sell_ptr, Am->d_sell_row, Am->d_sell_len, Am->d_sell_col,
+        static_cast<const V*>(Am->d_sell_val), x, y, Am->sell_slices, Am->nrows);
+    NM_CHECK_LAUNCH();
+    return NM_OK;
+}
+
+int build_sell(nm_csr* A) {
+    A->sell_tried = true;
+    const int32_t n = A->nrows;
+    const int32_t* rp = A->h_row_ptr.data();
+    std::vector<int32_t> perm(n), lens(n);
+    for (int32_t w0 = 0; w0 < n; w0 += kSellWindow) {
+        const int32_t w1 = std::min(n, w0 + kSellWindow);
+        for (int32_t i = w0; i < w1; ++i) perm[i] = i;
+        std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
+            return rp[a + 1] - rp[a] > rp[b + 1] - rp[b];
+        });
+    }
+    for (int32_t i = 0; i < n; ++i) lens[i] = rp[perm[i] + 1] - rp[perm[i]];
+    const int32_t ns = (n + 31) / 32;
+    std::vector<int64_t> sp(size_t(ns) + 1, 0);
+    for (int32_t s = 0; s < ns; ++s) {
+        int32_t w = 0;
+        for (int32_t i = s * 32; i < std::min(n, s * 32 + 32); ++i) w = std::max(w, lens[i]);
+        sp[s + 1] = sp[s] + 32 * int64_t(w);
+    }
+    const int64_t total = sp[ns];
+    // too much padding (a few very long rows among short ones): keep the
+    // per-group gather kernel
+    if (total > 2 * int64_t(A->nnz) + 32 * int64_t(kSellWindow)) return NM_OK;
+    A->sell_slices = ns;
+    NM_CUDA_TRY(cudaMalloc(&A->d_sell_ptr, sizeof(int64_t) * sp.size()));
+    NM_CUDA_TRY(cudaMalloc(&A->d_sell_row, sizeof(int32_t) * size_t(n)));
+    NM_CUDA_TRY(cudaMalloc(&A->d_sell_len, sizeof(int32_t) * size_t(n)));
+    NM_CUDA_TRY(cudaMemcpy(A->d_sell_ptr, sp.data(), sizeof(int64_t) * sp.size(),
+                           cudaMemcpyHostToDevice));
+    NM_CUDA_TRY(cudaMemcpy(A->d_sell_row, perm.data(), sizeof(int32_t) * size_t(n),
+                           cudaMemcpyHostToDevice));
+    NM_CUDA_TRY(cudaMemcpy(A->d_sell_len, lens.data(), sizeof(int32_t) * size_t(n),
+                           cudaMemcpyHostToDevice));
+    int st = NM_OK;
+    switch (A->dtype) {
+        case NM_F64: st = fill_sell<double>(A, total); break;
+        case NM_F32: st = fill_sell<float>(A, total); break;
+        default: st = fill_sell<__nv_bfloat16>(A, total); break;
+    }
+    if (st != NM_OK) return st;
+    A->sell_ready = true;
+    return NM_OK;
+}
+
 template <typename V, typename X, typename A, int TILE, int STAGES>
 static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     CsrView<V> M = Am->view<V>();
@@ -208,7 +392,8 @@ static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
 
 template <typename V, typename X, typename A>
 static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    if (Am->warp_gather) return launch_gather<V, X, A>(Am, x, y, s);
+    if (Am->warp_gather)
+        return Am->sell_ready ? launch_sell<V, X, A>(Am, x, y, s) : launch_gather<V, X, A>(Am, x, y, s);
     switch (Am->tune.tile) {
         case 1024: return launch_stages<V, X, A, 1024>(Am, x, y, s);
         case 2048: return launch_stages<V, X, A, 2048>(Am, x, y, s);

@@ -22,18 +22,28 @@ from . import generators as gen
 
 
 def make_requests(count: int, rate: float, seed: int = 4, side_range=(32, 1024),
-                  banded_range=(256, 65536)):
+                  banded_range=(256, 65536), pool: int | None = None):
     """The served workload: Poisson arrivals at `rate` req/s (rate <= 0: all at
     t = 0); each request with equal probability a 2-D 5-point Laplacian with
     side log-uniform in side_range, or a banded SPD matrix (half-bandwidth
     uniform in 1..8, 2 mirrored off-band entries per row, diagonal 1.05 x the
-    off-diagonal row sum) with n log-uniform in banded_range; b ~ N(0, 1)."""
+    off-diagonal row sum) with n log-uniform in banded_range; b ~ N(0, 1).
+
+    pool: when count exceeds it, only the first `pool` requests draw their own
+    system (A, b) -- an i.i.d. sample of the distribution -- and request i
+    reuses system i mod pool, while every request still draws its own arrival
+    time.  A 20,000-request stream would otherwise hold ~100 GB of host CSR
+    arrays.  The first `pool` requests are those of the unpooled stream."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
-    for _ in range(count):
+    for i in range(count):
         if rate > 0:
             t += rng.exponential(1.0 / rate)
+        if pool is not None and i >= pool:
+            _, A, b, kind = out[i % pool]
+            out.append((t, A, b, kind))
+            continue
         if rng.random() < 0.5:
             side = int(round(math.exp(rng.uniform(math.log(side_range[0]),
                                                   math.log(side_range[1])))))
