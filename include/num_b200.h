@@ -281,6 +281,14 @@ typedef struct {
                            solve's estimate (default 2; <= 0 keeps the default) */
 } nm_solver_opts;
 
+/* Process-wide choice of how a step's inner iterations run: 1 (default) one
+ * persistent cooperative launch per step (SpMV, update and p update of every
+ * live system separated by grid barriers, ending as soon as no system
+ * iterates), when the device supports it; 0 a CUDA graph whose loop body
+ * launches those phases as kernels.  Both give the same bits.  Other values:
+ * NM_ERR_INVALID. */
+int nm_solver_set_persistent(int32_t enable);
+
 /* A solver with a device arena for up to max_rows rows and max_nnz nonzeros
  * in total over max_systems concurrently resident systems. */
 int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_systems,

@@ -84,6 +84,7 @@ _SIGNATURES = {
     "nm_cg_local_static": ([vp, vp, vp, dbl, i32, C.POINTER(CgResult), vp], C.c_int),
     "nm_solver_create": ([i64, i64, i32, C.POINTER(SolverOpts), C.POINTER(vp)], C.c_int),
     "nm_solver_destroy": ([vp], C.c_int),
+    "nm_solver_set_persistent": ([i32], C.c_int),
     "nm_solver_admit": ([vp, vp, vp, vp, i32, vp, vp, dbl, i32, P_i32], C.c_int),
     "nm_solver_admit_batch": ([vp, i32, vp, vp, vp, vp, vp, dbl, i32, P_i32, P_i32], C.c_int),
     "nm_solver_step": ([vp, i32, P_i32], C.c_int),

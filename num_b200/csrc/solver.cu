@@ -36,6 +36,7 @@
 //   chunk of inner iterations, then reads every system's state; the host
 //   admits new systems and retires finished ones between steps.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -45,6 +46,7 @@
 #include <thread>
 #include <vector>
 
+#include "cg.cuh"
 #include "spmv.cuh"
 
 namespace nm {
@@ -81,6 +83,11 @@ struct ListHdr {
 // number, so the r.z parity of each iteration is fixed in the body).
 struct StepCtl {
     unsigned int iter, live, cap, pad_;
+    // the persistent step (bs_persist): its grid barrier, the systems still
+    // iterating after each iteration (alternating by iteration parity), and
+    // its failure flag
+    unsigned int bar_count, bar_gen, live2[2];
+    int32_t status, pad2_[3];
 };
 
 
@@ -243,6 +250,63 @@ __device__ __forceinline__ double2 ordered_sum_all(const double* part, int64_t l
     return block_sum2_all(sx, sy, scratch);
 }
 
+// The per-system sums of the inner iteration (alpha's p.Ap, beta's r.z and
+// r.r) in one order for every path: ordered_sum_all as a CTA of 256 threads
+// computes it.  Threads 256 and up (the producer warp of a persistent CTA)
+// add nothing; every thread of the CTA calls it and gets the result.
+// scratch: kWarps + 1 entries.
+template <bool PAIRS>
+__device__ __forceinline__ double2 ordered_sum256(const double* part, int64_t lo, int64_t hi,
+                                                  double2* scratch) {
+    double ax[8] = {0, 0, 0, 0, 0, 0, 0, 0}, ay[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    constexpr int64_t bs = kThreads;
+    auto ld = [&](int64_t i) -> double2 {
+        if (PAIRS) return __ldcg(reinterpret_cast<const double2*>(part) + i);
+        return make_double2(__ldcg(part + i), 0.0);
+    };
+    if (threadIdx.x < kThreads) {
+        int64_t i = lo + threadIdx.x;
+        for (; i + 7 * bs < hi; i += 8 * bs) {
+            double2 v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = ld(i + k * bs);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                ax[k] += v[k].x;
+                ay[k] += v[k].y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            const int64_t j = i + k * bs;
+            if (j < hi) {
+                const double2 v = ld(j);
+                ax[k] += v.x;
+                ay[k] += v.y;
+            }
+        }
+    }
+    double sx = ((ax[0] + ax[1]) + (ax[2] + ax[3])) + ((ax[4] + ax[5]) + (ax[6] + ax[7]));
+    double sy = ((ay[0] + ay[1]) + (ay[2] + ay[3])) + ((ay[4] + ay[5]) + (ay[6] + ay[7]));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    if (lane == 0 && warp < kWarps) scratch[warp] = make_double2(sx, sy);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < kWarps; ++w) {
+            t.x += scratch[w].x;
+            t.y += scratch[w].y;
+        }
+        scratch[kWarps] = t;
+    }
+    __syncthreads();
+    const double2 out = scratch[kWarps];
+    __syncthreads();  // scratch is free for the next call
+    return out;
+}
+
 // ---- per-system scalar steps (one CTA per system of the outer list) ----------------
 
 enum ScalarKind { kOuterNorm = 2, kStart = 3 };
@@ -312,31 +376,31 @@ __global__ void __launch_bounds__(kScalarThreads)
 // (after the SpMV), and the stopping test and beta from the tile sums (after
 // the update), one CTA per system; the same formulas as the tile kernels use
 // for small systems.
-__global__ void __launch_bounds__(kScalarThreads)
+// (256-thread CTAs: the sums are those every path forms, ordered_sum256.)
+__global__ void __launch_bounds__(kThreads)
     bs_alpha(const SysRef* list, const int32_t* count, SysState* sys, const double* part_blk,
              int par) {
-    __shared__ double2 red[kScalarThreads / 32 + 1];
+    __shared__ double2 red[kWarps + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const SysRef ref = list[i];
         SysState& S = sys[ref.slot];
         if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
-        const double pAp = ordered_sum_all<false>(part_blk, ref.blk0, ref.blk1, red).x;
+        const double pAp = ordered_sum256<false>(part_blk, ref.blk0, ref.blk1, red).x;
         if (threadIdx.x == 0) S.alpha = pAp != 0.0 ? __ldcg(&S.rzp[par]) / pAp : 0.0;
-        __syncthreads();  // red is reused by the next system
     }
 }
 
-__global__ void __launch_bounds__(kScalarThreads)
+__global__ void __launch_bounds__(kThreads)
     bs_beta(const SysRef* list, const int32_t* count, SysState* sys, const double* part_tile,
             int par, StepCtl* ctl) {
-    __shared__ double2 red[kScalarThreads / 32 + 1];
+    __shared__ double2 red[kWarps + 1];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const SysRef ref = list[i];
         SysState& S = sys[ref.slot];
         if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
-        const double2 t = ordered_sum_all<true>(part_tile, ref.tile0, ref.tile1, red);
+        const double2 t = ordered_sum256<true>(part_tile, ref.tile0, ref.tile1, red);
         if (threadIdx.x == 0) {
             const double inner_rel = sqrt(t.y / S.rr0);
             const double est = S.rnorm * sqrt(t.y) / S.bnorm;
@@ -471,57 +535,95 @@ __global__ void __launch_bounds__(kThreads)
 
 __host__ __device__ constexpr int kVecIters(int vn) { return kTileRows / (vn * kThreads); }
 
-// Inner iteration, step 2 (after the SpMV): alpha = r.z / p.Ap from the
-// system's block sums (every CTA of the system sums them, in the same order),
-// d += alpha p, r -= alpha Ap, z = M^-1 r, and the tile's (r.z, r.r) -> part.
-// The system's first tile counts the iteration.  No atomics: step 3 reduces
-// the tile sums.
-template <typename T>
-__global__ void __launch_bounds__(kThreads, 4)
-    bs_update(const int4* tiles, const int32_t* count, SysState* sys, const int2* sblk,
-              const int2* stile, const double* part_blk, const T* __restrict__ p,
-              const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
-              T* __restrict__ z, T* __restrict__ d, double* part_tile, int par) {
+// Loads of the vector steps.  COH: the data may have been written earlier in
+// the same launch (the persistent step), so it is read through L2
+// (ld.global.cg), never from a possibly stale L1 line.
+template <typename T, bool COH>
+__device__ __forceinline__ void vload_c(const T* p, int64_t row, T (&v)[Vec16<T>::N]) {
+    using VT = typename Vec16<T>::type;
+    VT q;
+    if constexpr (COH)
+        q = __ldcg(reinterpret_cast<const VT*>(p + row));
+    else
+        q = *reinterpret_cast<const VT*>(p + row);
+    memcpy(v, &q, sizeof q);
+}
+
+// Sums of two values over the first 8 warps (256 threads) in warp order, to
+// every thread: block_sum2_all as a 256-thread CTA forms it.
+__device__ __forceinline__ double2 block_sum2_8(double a, double b, double2* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0 && warp < kWarps) scratch[warp] = make_double2(a, b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < kWarps; ++w) {
+            t.x += scratch[w].x;
+            t.y += scratch[w].y;
+        }
+        scratch[kWarps] = t;
+    }
+    __syncthreads();
+    const double2 out = scratch[kWarps];
+    __syncthreads();
+    return out;
+}
+
+// Inner iteration, step 2 (after the SpMV), for tile i: alpha = r.z / p.Ap
+// from the system's block sums (every CTA of the system sums them, in the same
+// order), d += alpha p, r -= alpha Ap, z = M^-1 r, and the tile's (r.z, r.r)
+// -> part.  The system's first tile counts the iteration.  No atomics: step 3
+// reduces the tile sums.  Threads 0..255 of the CTA carry the tile; every
+// thread calls it.  SELF: a large system's alpha is reduced here too, in the
+// same order bs_alpha uses, instead of read from bs_alpha.
+template <typename T, bool COH, bool SELF>
+__device__ __forceinline__ void update_tile(int32_t i, const int4 tl, SysState* sys,
+                                            const int2* sblk, const int2* stile,
+                                            const double* part_blk, const T* __restrict__ p,
+                                            const T* __restrict__ Ap, const T* __restrict__ dinv,
+                                            T* __restrict__ r, T* __restrict__ z,
+                                            T* __restrict__ d, double* part_tile, int par,
+                                            double2* red) {
     constexpr int VN = Vec16<T>::N;
     constexpr int IT = kVecIters(VN);
-    __shared__ double2 red[kWarps + 1];
-    const int32_t i = blockIdx.x;
-    if (i >= __ldcg(count)) return;
-    const int4 tl = tiles[i];
     const int32_t slot = tl.z;
+    const bool mine = threadIdx.x < kThreads;
     T rz = T(0), rr = T(0);
-    if (sys_phase(sys, slot) == kSysInner) {  // phase is not written by this kernel
+    if (sys_phase(sys, slot) == kSysInner) {  // phase is not written in this step
         double alpha_d;
-        if (tl.w) {  // large system: bs_alpha reduced it
+        if (tl.w && !SELF) {  // large system: bs_alpha reduced it
             alpha_d = __ldcg(&sys[slot].alpha);
-        } else {  // small system: at most a few block sums per thread
+        } else {  // every CTA of the system sums its block sums in the same order
             const int2 br = __ldg(sblk + slot);
-            const double pAp = ordered_sum_all<false>(part_blk, br.x, br.y, red).x;
+            const double pAp = ordered_sum256<false>(part_blk, br.x, br.y, red).x;
             const double rz_old = __ldcg(&sys[slot].rzp[par]);
             alpha_d = pAp != 0.0 ? rz_old / pAp : 0.0;
         }
         const T alpha = T(alpha_d);
         // vectors of each operand per thread in flight at a time (within 64
-        // registers): two for FP32, one for FP64
-        constexpr int KB = sizeof(T) == 4 ? (IT < 2 ? IT : 2) : 1;
+        // registers): two for FP32, one for FP64 -- and one in the persistent
+        // step, whose CTAs also hold the SpMV pipeline's registers
+        constexpr int KB = (sizeof(T) == 4 && !COH) ? (IT < 2 ? IT : 2) : 1;
 #pragma unroll
         for (int k0 = 0; k0 < IT; k0 += KB) {
             T pv[KB][VN], av[KB][VN], rv[KB][VN], dv[KB][VN], mv[KB][VN];
 #pragma unroll
             for (int k = 0; k < KB; ++k) {
                 const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
-                if (row < tl.y) {
-                    vload(p, row, pv[k]);
-                    vload(Ap, row, av[k]);
-                    vload(r, row, rv[k]);
-                    vload(d, row, dv[k]);
-                    vload(dinv, row, mv[k]);
+                if (mine && row < tl.y) {
+                    vload_c<T, COH>(p, row, pv[k]);
+                    vload_c<T, COH>(Ap, row, av[k]);
+                    vload_c<T, COH>(r, row, rv[k]);
+                    vload_c<T, COH>(d, row, dv[k]);
+                    vload_c<T, false>(dinv, row, mv[k]);
                 }
             }
 #pragma unroll
             for (int k = 0; k < KB; ++k) {
                 const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
-                if (row < tl.y) {
+                if (mine && row < tl.y) {
                     const int valid = int(min(int64_t(VN), int64_t(tl.y) - row));
                     T zo[VN];
 #pragma unroll
@@ -545,39 +647,50 @@ __global__ void __launch_bounds__(kThreads, 4)
             sys[slot].it_total += 1;
         }
     }
-    const double2 t = block_sum2_all(double(rz), double(rr), red);
+    const double2 t = block_sum2_8(double(rz), double(rr), red);
     if (threadIdx.x == 0) reinterpret_cast<double2*>(part_tile)[i] = t;
 }
 
-// Inner iteration, step 3: (r.z, r.r) of the system from its tile sums
-// (every CTA, same order); the inner stopping test; p = z + beta p with
-// beta = r.z / previous r.z.  r.z alternates between rzp[par] (read) and
-// rzp[par ^ 1] (written by the system's first tile), so no CTA reads a value
-// another CTA of this launch writes; the phase change of a stopping system is
-// the one write others may see early, and they then skip exactly as the test
-// would make them.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
-    bs_pupdate(const int4* tiles, const int32_t* count, SysState* sys, const int2* stile,
-               const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par,
-               StepCtl* ctl) {
-    constexpr int VN = Vec16<T>::N;
-    constexpr int IT = kVecIters(VN);
+    bs_update(const int4* tiles, const int32_t* count, SysState* sys, const int2* sblk,
+              const int2* stile, const double* part_blk, const T* __restrict__ p,
+              const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
+              T* __restrict__ z, T* __restrict__ d, double* part_tile, int par) {
     __shared__ double2 red[kWarps + 1];
-    __shared__ int32_t phase;
     const int32_t i = blockIdx.x;
     if (i >= __ldcg(count)) return;
-    const int4 tl = tiles[i];
+    update_tile<T, false, false>(i, tiles[i], sys, sblk, stile, part_blk, p, Ap, dinv, r, z, d,
+                                 part_tile, par, red);
+}
+
+// Inner iteration, step 3, for tile i: (r.z, r.r) of the system from its tile
+// sums (every CTA, same order); the inner stopping test; p = z + beta p with
+// beta = r.z / previous r.z.  r.z alternates between rzp[par] (read) and
+// rzp[par ^ 1] (written by the system's first tile), so no CTA reads a value
+// another CTA of this step writes; the phase change of a stopping system is
+// the one write others may see early, and they then skip exactly as the test
+// would make them.  A continuing system's first tile counts it in *live.
+// SELF: a large system is decided here too, in bs_beta's order.
+template <typename T, bool COH, bool SELF>
+__device__ __forceinline__ void pupdate_tile(int32_t i, const int4 tl, SysState* sys,
+                                             const int2* stile, const double* part_tile,
+                                             const T* __restrict__ z, T* __restrict__ p, int par,
+                                             unsigned int* live, double2* red, int32_t* sh) {
+    constexpr int VN = Vec16<T>::N;
+    constexpr int IT = kVecIters(VN);
     const int32_t slot = tl.z;
-    if (threadIdx.x == 0) phase = sys_phase(sys, slot);
+    if (threadIdx.x == 0) *sh = sys_phase(sys, slot);
     __syncthreads();
+    const int32_t phase = *sh;
+    __syncthreads();  // *sh is free for the next tile
     if (phase != kSysInner) return;  // uniform over the CTA
     double beta_d;
-    if (tl.w) {  // large system: bs_beta ran the test and set beta (phase above)
+    if (tl.w && !SELF) {  // large system: bs_beta ran the test and set beta (phase above)
         beta_d = __ldcg(&sys[slot].beta);
-    } else {  // small system: reduce the tile sums and decide, as every CTA of it does
+    } else {  // reduce the tile sums and decide, as every CTA of the system does
         const int2 tr = __ldg(stile + slot);
-        const double2 t = ordered_sum_all<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
+        const double2 t = ordered_sum256<true>(part_tile, tr.x, tr.y, red);  // (r.z, r.r)
         const SysState& S = sys[slot];
         const double rr0 = __ldcg(&S.rr0), rnorm = __ldcg(&S.rnorm), bnorm = __ldcg(&S.bnorm);
         const double inner_rel = sqrt(t.y / rr0);
@@ -600,12 +713,14 @@ __global__ void __launch_bounds__(kThreads, 4)
             sys[slot].rr = t.y;
             sys[slot].beta = beta_d;
             sys[slot].rzp[par ^ 1] = t.x;
-            if (ctl) atomicAdd(&ctl->live, 1u);
+            if (live) atomicAdd(live, 1u);
         }
     }
+    if (threadIdx.x >= kThreads) return;
     const T beta = T(beta_d);
-    // four vectors of each operand per thread in flight at a time
-    constexpr int KB = IT < 4 ? IT : 4;
+    // four vectors of each operand per thread in flight at a time (two in the
+    // persistent step)
+    constexpr int KB = COH ? (IT < 2 ? IT : 2) : (IT < 4 ? IT : 4);
 #pragma unroll
     for (int k0 = 0; k0 < IT; k0 += KB) {
         T zv[KB][VN], pv[KB][VN];
@@ -613,8 +728,8 @@ __global__ void __launch_bounds__(kThreads, 4)
         for (int k = 0; k < KB; ++k) {
             const int64_t row = tl.x + int64_t(VN) * (threadIdx.x + (k0 + k) * kThreads);
             if (row < tl.y) {
-                vload(z, row, zv[k]);
-                vload(p, row, pv[k]);
+                vload_c<T, COH>(z, row, zv[k]);
+                vload_c<T, COH>(p, row, pv[k]);
             }
         }
 #pragma unroll
@@ -628,6 +743,118 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 4)
+    bs_pupdate(const int4* tiles, const int32_t* count, SysState* sys, const int2* stile,
+               const double* part_tile, const T* __restrict__ z, T* __restrict__ p, int par,
+               StepCtl* ctl) {
+    __shared__ double2 red[kWarps + 1];
+    __shared__ int32_t sh;
+    const int32_t i = blockIdx.x;
+    if (i >= __ldcg(count)) return;
+    pupdate_tile<T, false, false>(i, tiles[i], sys, stile, part_tile, z, p, par,
+                                  ctl ? &ctl->live : nullptr, red, &sh);
+}
+
+// ---- the persistent step: the whole iteration loop in one cooperative launch ----------
+//
+// Every CTA of a co-resident grid runs the step's iterations itself: the SpMV
+// pipeline over the inner block list (PhaseGate, InnerEpi), then the update of
+// the tiles blockIdx.x, + gridDim.x, ..., then their p update, with a bounded
+// grid barrier after each phase -- the three phases the graph path launches as
+// kernels, with the same per-block / per-tile sums and the same per-system
+// reductions (ordered_sum256, also for large systems, whose alpha / beta the
+// graph path reduces in bs_alpha / bs_beta in the same order), so the two
+// paths give the same bits.  Data written inside the launch is read through
+// L2.  After the third barrier every CTA reads how many systems go on (counted
+// by their first tiles into live2[parity]); the loop ends when none does or at
+// the step's cap.  A wait that gives up sets the error word and ctl->status,
+// and every CTA leaves at its next barrier.
+
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+template <typename T>
+struct InnerEpiCoherent {  // InnerEpi reading p through L2
+    static constexpr bool kBlockSums = true;
+    T* __restrict__ Ap;
+    const T* __restrict__ p;
+    double* __restrict__ part;
+    T acc;
+    __device__ __forceinline__ void operator()(int32_t row, T v) {
+        Ap[row] = v;
+        acc += __ldcg(p + row) * v;
+    }
+    __device__ __forceinline__ double take() {
+        const double a = double(acc);
+        acc = T(0);
+        return a;
+    }
+    __device__ __forceinline__ void finish_block(int64_t b, const BlockDesc&, double sum) {
+        part[b] = sum;
+    }
+};
+
+template <typename V, typename T>
+__global__ void __launch_bounds__(kCtaThreads, 2)
+    bs_persist(CsrView<V> M, T* p, T* Ap, const T* dinv, T* r, T* z, T* d, SysState* sys,
+               const int4* tiles, const int32_t* tile_count, const int2* sblk, const int2* stile,
+               double* part_blk, double* part_tile, StepCtl* ctl, unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<V, T, T, kSolverTile, kSolverStages>*>(smem_raw);
+    __shared__ double2 red[kWarps + 1];
+    __shared__ int32_t sh;
+    __shared__ bool flag;
+    const int t = threadIdx.x;
+    const unsigned int cap = __ldcg(&ctl->cap);
+    M.coherent_x = 1;
+    unsigned int it = 0;
+    bool failed = false;
+    while (it < cap) {
+        const int par = int(it & 1u);
+        fence_proxy_async_global();  // p written by the previous iteration, then read by TMA
+        InnerEpiCoherent<T> epi{Ap, p, part_blk, T(0)};
+        const bool ok = spmv_pipeline<V, T, T, kSolverTile, kSolverStages>(
+            M, p, sm, epi, err, PhaseGate{sys, kSysInner});
+        __syncthreads();
+        if (t == 0) {  // the ring's barriers are initialised again by the next SpMV
+#pragma unroll
+            for (int q = 0; q < kSolverStages; ++q) {
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&sm.full[q]))
+                             : "memory");
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&sm.empty[q]))
+                             : "memory");
+            }
+        }
+        if (!ok) atomicExch(&ctl->status, kCgDeviceError);
+        if (!grid_barrier(&ctl->bar_count, &ctl->bar_gen, err, &ctl->status, &flag)) {
+            failed = true;
+            break;
+        }
+        if (blockIdx.x == 0 && t == 0) ctl->live2[par ^ 1] = 0u;  // read before the last barrier
+        const int32_t ntile = __ldcg(tile_count);
+        for (int32_t i = blockIdx.x; i < ntile; i += gridDim.x)
+            update_tile<T, true, true>(i, tiles[i], sys, sblk, stile, part_blk, p, Ap, dinv, r, z,
+                                       d, part_tile, par, red);
+        if (!grid_barrier(&ctl->bar_count, &ctl->bar_gen, err, &ctl->status, &flag)) {
+            failed = true;
+            break;
+        }
+        for (int32_t i = blockIdx.x; i < ntile; i += gridDim.x)
+            pupdate_tile<T, true, true>(i, tiles[i], sys, stile, part_tile, z, p, par,
+                                        &ctl->live2[par], red, &sh);
+        if (!grid_barrier(&ctl->bar_count, &ctl->bar_gen, err, &ctl->status, &flag)) {
+            failed = true;
+            break;
+        }
+        ++it;
+        if (__ldcg(&ctl->live2[par]) == 0u) break;  // the same value in every CTA
+    }
+    if (failed && t == 0) atomicExch(&ctl->status, kCgDeviceError);
+    if (blockIdx.x == 0 && t == 0) ctl->iter = it;
 }
 
 constexpr int kLoopUnroll = 8;  // iterations per body of a step's loop
@@ -750,6 +977,7 @@ struct nm_solver {
     nm::StepCtl* ctl = nullptr;    // device control words of the step loop
     nm::StepCtl* h_ctl = nullptr;  // pinned: the cap going in, the counts coming back
     int grid_spmv_inner = 0, grid_spmv_outer = 0, grid_vec = 0, grid_scalar = 0;
+    int grid_persist = 0;     // co-resident grid of bs_persist (0: not available)
     int64_t lists_gen = 0;   // bumped when the work-list arrays are reallocated
     int64_t graph_gen = -1;  // lists_gen the step graph was built against
     int graph_tiles = 0;     // tile grid of the step graph
@@ -968,13 +1196,13 @@ int launch_inner_body(nm_solver* S, cudaGraphConditionalHandle loop) {
         StepCtl* ctl = it == kLoopUnroll - 1 ? S->ctl : nullptr;
         bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
                                                               S->err);
-        if (g_big) bs_alpha<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                             S->part_blk, par);
+        if (g_big) bs_alpha<<<g_big, kThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                       S->part_blk, par);
         bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->sblk, S->stile,
                                                 S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
                                                 par);
-        if (g_big) bs_beta<<<g_big, kScalarThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                            S->part_tile, par, ctl);
+        if (g_big) bs_beta<<<g_big, kThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                      S->part_tile, par, ctl);
         bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
                                                  S->part_tile, z, p, par, ctl);
     }
@@ -1033,8 +1261,48 @@ int prepare_solver_kernels(nm_solver* S) {
     S->grid_spmv_outer = sm_count() * occ;
     S->grid_vec = sm_count() * 4;
     S->grid_scalar = sm_count() * 2;
+    int dev = 0, coop = 0;
+    NM_CUDA_TRY(cudaGetDevice(&dev));
+    NM_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    S->grid_persist = 0;
+    if (coop) {
+        st = prepare_kernel(reinterpret_cast<const void*>(bs_persist<V, T>), kCtaThreads,
+                            spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), &occ);
+        if (st != NM_OK) return st;
+        S->grid_persist = sm_count() * occ;
+    }
     return NM_OK;
 }
+
+// The step loop as one cooperative launch (bs_persist).
+template <typename V, typename T>
+int launch_persist(nm_solver* S) {
+    const ListHdr* H = S->hdr;
+    CsrView<V> M = arena_view<V>(S, S->vin ? S->vin : S->v64, S->iblk, &H->iblk);
+    T* p = static_cast<T*>(S->p);
+    T* Ap = static_cast<T*>(S->Ap);
+    const T* dinv = static_cast<const T*>(S->dinv);
+    T* r = static_cast<T*>(S->r);
+    T* z = static_cast<T*>(S->z);
+    T* d = static_cast<T*>(S->d);
+    SysState* sys = S->st;
+    const int4* tiles = S->itile;
+    const int32_t* tcount = &H->itile;
+    const int2* sblk = S->sblk;
+    const int2* stile = S->stile;
+    double* pb = S->part_blk;
+    double* pt = S->part_tile;
+    StepCtl* ctl = S->ctl;
+    unsigned int* err = S->err;
+    void* args[] = {&M,    &p,     &Ap,    &dinv, &r,  &z,  &d,   &sys,
+                    &tiles, &tcount, &sblk, &stile, &pb, &pt, &ctl, &err};
+    NM_CUDA_TRY(cudaLaunchCooperativeKernel(
+        reinterpret_cast<const void*>(bs_persist<V, T>), dim3(S->grid_persist), dim3(kCtaThreads),
+        args, spmv_smem_bytes<V, T, T, kSolverTile, kSolverStages>(), S->stream));
+    return NM_OK;
+}
+
+std::atomic<int> g_engine_persistent{1};  // nm_solver_set_persistent
 
 // FP64 -> BF16 through FP32, round to nearest even, NaN kept quiet; written
 // without branches so the loop vectorises.
@@ -1144,6 +1412,14 @@ extern "C" int nm_solver_create(int64_t max_rows, int64_t max_nnz, int32_t max_s
     }
     if (st != NM_OK) return st;
     *out = S.release();
+    return NM_OK;
+}
+
+extern "C" int nm_solver_set_persistent(int32_t enable) {
+    nm::clear_error();
+    if (enable != 0 && enable != 1)
+        return fail(NM_ERR_INVALID, "nm_solver_set_persistent: 0 or 1");
+    nm::g_engine_persistent.store(enable);
     return NM_OK;
 }
 
@@ -1571,7 +1847,20 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
         S->ctr.outer_launches += 1;
     }
     lap(S->ctr.s_outer);
-    if (iters > 0) {
+    if (iters > 0 && S->grid_persist > 0 && g_engine_persistent.load()) {
+        // the whole loop in one cooperative launch
+        *S->h_ctl = StepCtl{};
+        S->h_ctl->cap = unsigned(iters);
+        NM_CUDA_TRY(cudaMemcpyAsync(S->ctl, S->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice,
+                                    S->stream));
+        switch (S->inner) {
+            case NM_F64: st = launch_persist<double, double>(S); break;
+            case NM_F32: st = launch_persist<float, float>(S); break;
+            default: st = launch_persist<__nv_bfloat16, float>(S); break;
+        }
+        if (st != NM_OK) return st;
+        S->step_loops = true;
+    } else if (iters > 0) {
         const bool big = S->h_hdr->bsys > 0;
         const int tiles = tile_bucket(S->h_hdr->itile);
         if (!S->chunk_valid || S->graph_big != big || S->graph_tiles != tiles ||
@@ -1640,7 +1929,8 @@ extern "C" int nm_solver_step_begin(nm_solver* S, int32_t iters) {
             S->graph_gen = S->lists_gen;
         }
         lap(S->ctr.s_capture);
-        *S->h_ctl = StepCtl{0u, 0u, unsigned(iters), 0u};
+        *S->h_ctl = StepCtl{};
+        S->h_ctl->cap = unsigned(iters);
         NM_CUDA_TRY(cudaMemcpyAsync(S->ctl, S->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice,
                                     S->stream));
         NM_CUDA_TRY(cudaGraphLaunch(S->chunk_exec, S->stream));

@@ -249,3 +249,31 @@ def test_take_many_matches_take(kspmv):
     for (xa, ia), (xb, ib) in zip(one, many):
         assert ia == ib and np.array_equal(xa, xb)
     assert S2.info()["free_slots"] == 16
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+def test_persistent_step_equals_graph_step(kspmv, nmlib, precision):
+    # The step loop in one cooperative launch (grid barriers between the SpMV,
+    # update and p-update phases) and the CUDA-graph loop of kernels give the
+    # same bits and iteration counts, for a mix of small banded systems and a
+    # large Laplacian (more than 512 row blocks: its alpha / beta reduced by
+    # bs_alpha / bs_beta on the graph path, in-CTA on the persistent one).
+    mats, _ = gen.banded_batch(24, seed=8)
+    rng = np.random.default_rng(9)
+    systems = [(A, rng.standard_normal(A.nrows)) for A in mats]
+    L = gen.laplacian_2d(400)
+    systems.insert(7, (L, rng.standard_normal(L.nrows)))
+    out = []
+    try:
+        for mode in (1, 0, 1):
+            nmlib.nm_solver_set_persistent(mode)
+            S = _solver(precision, rows=1_000_000, nnz=6_000_000, systems=64)
+            out.append(S.solve(systems, tol=1e-9, max_iter=20000, chunk=16))
+            del S
+    finally:
+        nmlib.nm_solver_set_persistent(1)
+    for run in out[1:]:
+        for (xa, ia), (xb, ib) in zip(out[0], run):
+            assert ia == ib and np.array_equal(xa, xb)
+    for (A, b), (x, info) in zip(systems, out[0]):
+        assert info["converged"] and _true_rel(A, x, b) < 1e-9
