@@ -565,10 +565,14 @@ def run_batch(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e_ms = max_over_ranks([e0.elapsed_time(e1) / e_steps], world, dev)[0]
+    lib_ref = cusparse_spmm_reference(A, X, dev, stream)
     if rank != 0:
         return None
     peak, peak_src = measured_peak()
     achieved = nbytes / (kern_avg_ms * 1e-3) / 1e9
+    if "us" in lib_ref:
+        lib_ref["gbs"] = round(nbytes / (lib_ref["us"] * 1e-6) / 1e9, 1)
+        lib_ref["library_us_over_ours"] = round(lib_ref["us"] / (kern_avg_ms * 1e3), 3)
     config = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz, "k": k,
               "bytes_per_step": nbytes,
               "bytes_formula": "12*nnz + 4*(n+1) + 8*k*(ncols + nrows)",
@@ -595,10 +599,39 @@ def run_batch(args, rank, world, local_rank):
                       "unit": "GB/s",
                       "note": "back-to-back steps right before the timed region, inside the "
                               "clock sampler's window"},
+        "library_reference": lib_ref,
     })
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_batch(A, k, budget_s=args.cpu_seconds)
     return line
+
+
+def cusparse_spmm_reference(A, X, dev, stream, steps=20):
+    """The library the reference's batch_spmv calls for k >= 32 (cuSPARSE
+    SpMM through KokkosKernels, src/batch_spmv_kernel.hpp:157-170), timed on
+    the same matrix and X: torch's CSR @ dense product, which runs cuSPARSE
+    SpMM.  Reported beside our kernel; not used on our path."""
+    import torch
+    try:
+        S = torch.sparse_csr_tensor(torch.tensor(A.row_ptr.astype(np.int64), device=dev),
+                                    torch.tensor(A.col_idx.astype(np.int64), device=dev),
+                                    torch.tensor(A.values, device=dev),
+                                    size=(A.nrows, A.ncols))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                Y = S @ X
+            e0.record(stream)
+            for _ in range(steps):
+                Y = S @ X
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return {"us": round(e0.elapsed_time(e1) * 1e3 / steps, 2),
+                "what": "cuSPARSE SpMM via torch.sparse_csr_tensor @ dense (the library "
+                        "KokkosKernels calls for k >= 32), same matrix and X",
+                "output_contiguous": bool(Y.is_contiguous())}
+    except Exception as e:  # the comparison is optional
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def cpu_baseline_batch(A, k, budget_s=10.0):

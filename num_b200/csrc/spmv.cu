@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // One warp per row (k wide enough for the row's columns to span the warp),
-// rows strided by the number of resident warps.  The warp reads a row's first
+// each CTA over its own contiguous range of rows.  The warp reads a row's first
 // 32 columns and values in one coalesced access, one row ahead, and its
 // row_ptr entries two rows ahead, so the row's X loads are the only memory
 // latency on its critical path; later 32-nonzero windows of longer rows are
@@ -550,9 +550,15 @@ __global__ void __launch_bounds__(kBatchWarpThreads)
                            const double* __restrict__ X, double* __restrict__ Y) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int64_t nw = int64_t(gridDim.x) * (kBatchWarpThreads / 32);
-    int64_t row = (int64_t(blockIdx.x) * kBatchWarpThreads + threadIdx.x) >> 5;  // same for the warp
-    if (row >= nrows) return;
+    // CTA b owns the contiguous rows [r_beg, r_end) and its warps take them in
+    // turn, so the X rows that neighbouring rows share (the band of the
+    // matrix) are read by one SM close together in time and reused from L1.
+    const int64_t per = (int64_t(nrows) + gridDim.x - 1) / gridDim.x;
+    const int64_t r_beg = int64_t(blockIdx.x) * per;
+    const int64_t r_end = r_beg + per < nrows ? r_beg + per : nrows;
+    const int64_t nw = kBatchWarpThreads / 32;
+    int64_t row = r_beg + (threadIdx.x >> 5);  // same for the warp
+    if (row >= r_end) return;
     int32_t s0 = __ldg(rp + row), s1 = __ldg(rp + row + 1);
     int32_t c_nx = 0;
     double v_nx = 0.0;
@@ -561,12 +567,12 @@ __global__ void __launch_bounds__(kBatchWarpThreads)
         v_nx = __ldg(vals + s0 + lane);
     }
     int32_t t0 = 0, t1 = 0;  // row_ptr entries of the next row
-    if (row + nw < nrows) {
+    if (row + nw < r_end) {
         t0 = __ldg(rp + row + nw);
         t1 = __ldg(rp + row + nw + 1);
     }
     const int pass_cols = 32 * VEC * CH;
-    for (; row < nrows; row += nw) {
+    for (; row < r_end; row += nw) {
         const int32_t r_s0 = s0, r_s1 = s1;
         const int32_t c_first = c_nx;
         const double v_first = v_nx;
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(kBatchWarpThreads)
             c_nx = __ldg(ci + s0 + lane);
             v_nx = __ldg(vals + s0 + lane);
         }
-        if (row + 2 * nw < nrows) {
+        if (row + 2 * nw < r_end) {
             t0 = __ldg(rp + row + 2 * nw);
             t1 = __ldg(rp + row + 2 * nw + 1);
         }
