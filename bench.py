@@ -372,6 +372,10 @@ def run_spmv(args, rank, world, local_rank):
         tuned = {k: at[k] for k in ("tile", "max_rows", "short_max", "grid_mult", "stages",
                                     "kernel")}
         tuned["chosen_by"] = f"autotune ({len(at['trials'])} candidates timed)"
+        best = {}
+        for tr in at["trials"]:
+            best[tr["kernel"]] = min(best.get(tr["kernel"], float("inf")), tr["us"])
+        tuned["best_us_by_kernel"] = best
     dt = torch.float64 if precision == "fp64" else torch.float32
     xd = torch.tensor(x, dtype=dt, device=dev)
     yd = torch.empty(A.nrows, dtype=dt, device=dev)
@@ -713,9 +717,19 @@ def cg_c1_measure(dev, steps, warmup, with_clock=True, local_rank=0):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e_ms = e0.elapsed_time(e1) / e_steps
+    from num_b200 import _lib
+    path = C.c_int32(-1)
+    _lib.load().nm_cg_last_path(M._h, C.byref(path))
     return {"A": A, "ms": ms, "iters": iters, "info": info, "max_err_vs_ones": err,
             "e2e_ms": e_ms, "h2d": bp.numel() * 8, "d2h": xp.numel() * 8,
-            "clocks": clk.summary() if clk else None}
+            "clocks": clk.summary() if clk else None, "path": CG_PATHS.get(path.value)}
+
+
+CG_PATHS = {0: "CUDA-graph chunks of 3 kernels per iteration",
+            1: "persistent TMA-pipelined solve, 3 grid barriers per iteration",
+            2: "persistent TMA-pipelined solve, 2 grid barriers per iteration",
+            3: "resident solve (matrix rows and vectors on chip, 2 grid-wide sums per "
+               "iteration)"}
 
 
 def run_cg(args, rank, world, local_rank):
@@ -740,8 +754,8 @@ def run_cg(args, rank, world, local_rank):
               "l2": "operands fit L2 (11.5 MB): L2 flushed before every solve, solves timed "
                     "alone; within a solve the iterations are L2-resident and latency-bound",
               "parallelism": f"replicas x{world}",
-              "api": "kokkos_spmv.cg_solve_local (C ABI nm_cg_local): 3 kernels per iteration "
-                     "in CUDA graph chunks"}
+              "api": "kokkos_spmv.cg_solve_local (C ABI nm_cg_local)",
+              "path": r["path"], "cg_mode": args.cg_mode}
     line = base_line(args, world, round(world * 1e3 / ms_per, 3), "solves/s", ms_per, precision,
                      config)
     line.update({
@@ -836,7 +850,8 @@ def run_engine(args, rank, world, local_rank):
               "iterations_enqueued_per_solve": its, "residual": st["residual"],
               "true_residual_fp64": true_res, "converged": st["converged"],
               "rel_error_vs_fp64_solution": err_fp64,
-              "chunk": chunk, "parallelism": f"replicas x{world}",
+              "chunk": chunk, "engine_mode": args.engine_mode,
+              "parallelism": f"replicas x{world}",
               "api": "num_b200.solver.BatchSolver (C ABI nm_solver_*): admit once, "
                      "nm_solver_resolve + steps per solve",
               "l2": "inputs larger than L2 (%.0f MB of matrix values + indices)" %
@@ -1320,6 +1335,12 @@ def main():
                     help="serve_c5: the engine's preconditioner")
     ap.add_argument("--no-plain", action="store_true",
                     help="serve_c5: skip the plain FP64 drop-in comparison")
+    ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2],
+                    help="nm_cg_set_persistent: 1 resident / persistent (default), 2 the "
+                         "TMA-pipelined persistent solve only, 0 CUDA-graph chunks")
+    ap.add_argument("--engine-mode", default="persistent", choices=["persistent", "graph"],
+                    help="nm_solver_set_persistent: one cooperative launch per engine step, or "
+                         "a CUDA graph of kernels")
     args = ap.parse_args()
     kind = WORKLOADS[args.workload][1]
     if args.steps <= 0:
@@ -1339,8 +1360,12 @@ def main():
         return
     import torch
     torch.cuda.set_device(local_rank)
+    from num_b200 import _lib
     from num_b200 import kokkos_spmv as kspmv
     kspmv.init(local_rank)
+    _lib.check(_lib.load().nm_cg_set_persistent(args.cg_mode), "nm_cg_set_persistent")
+    _lib.check(_lib.load().nm_solver_set_persistent(1 if args.engine_mode == "persistent" else 0),
+               "nm_solver_set_persistent")
     if world > 1:
         import datetime
 

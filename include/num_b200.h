@@ -231,6 +231,12 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
  * NM_ERR_INVALID.  No reference counterpart (an implementation switch). */
 int nm_cg_set_persistent(int32_t enable);
 
+/* How the last nm_cg_local / nm_dist_cg_single solve on A iterated: 0 the
+ * CUDA-graph chunks, 1 the TMA-pipelined persistent solve (three grid
+ * barriers per iteration), 2 the same in its two-barrier form, 3 the resident
+ * solve; -1 before A's first solve.  No reference counterpart. */
+int nm_cg_last_path(const nm_csr* A, int32_t* path);
+
 /* cg_solve_local (src/cg_solver.hpp:133-196; src/bindings.cpp:273-290):
  * unpreconditioned CG, x in/out, same stopping rule and iteration count.
  * The iteration runs on the device with device-resident scalars; the

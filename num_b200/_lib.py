@@ -68,6 +68,7 @@ _SIGNATURES = {
     "nm_csr_set_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
     "nm_csr_get_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
     "nm_cg_set_persistent": ([i32], C.c_int),
+    "nm_cg_last_path": ([vp, P_i32], C.c_int),
     "nm_csr_autotune": ([vp, vp, vp, vp, C.c_double, C.POINTER(Tuning), vp, i32, P_i32], C.c_int),
     "nm_csr_row_blocks": ([vp, vp, i32, vp], C.c_int),
     "nm_row_blocks_host": ([vp, i32, C.POINTER(Tuning), vp, i32, vp, P_i32], C.c_int),

@@ -659,11 +659,13 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
         // the whole iteration loop in one persistent launch
         st = resident ? launch_resident(A, ws, s) : launch_coop(A, ws, s);
         if (st != NM_OK) return st;
+        ws->last_path = resident ? 3 : (ws->coop_formed ? 2 : 1);
         NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         NM_CUDA_TRY(cudaStreamSynchronize(s));
     }
     // Otherwise iterate in graph chunks of growing length; poll `done` in between.
     int chunk = 8;
+    if (!coop) ws->last_path = 0;
     for (; !coop;) {
         NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         NM_CUDA_TRY(cudaStreamSynchronize(s));
@@ -688,6 +690,13 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
 }
 
 }  // namespace nm
+
+extern "C" int nm_cg_last_path(const nm_csr* A, int32_t* path) {
+    nm::clear_error();
+    if (!A || !path) return nm::fail(NM_ERR_INVALID, "nm_cg_last_path: NULL argument");
+    *path = A->cg ? A->cg->last_path : -1;
+    return NM_OK;
+}
 
 extern "C" int nm_cg_set_persistent(int32_t enable) {
     nm::clear_error();

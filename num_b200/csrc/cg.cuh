@@ -50,6 +50,7 @@ struct CgWorkspace {
     std::map<int, cudaGraphExec_t> graphs;  // iterations per graph -> exec
     // the resident solve (cg_resident.cu), when the matrix qualifies
     bool resident = false;
+    int32_t last_path = -1;  // path of the last solve (nm_cg_last_path)
     int res_tiles = 0, res_grid = 0, res_width = 0;
     size_t res_smem = 0;
     void* res_mem = nullptr;      // per-CTA row / window ranges and the sum slots

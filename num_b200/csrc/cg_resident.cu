@@ -18,7 +18,8 @@
 //    rows' new p (one of two alternating buffers) and, in the second half, r.
 //  * The two dot products per iteration are the grid's only synchronisation:
 //    each CTA publishes one sum per tile into a slot array with a release
-//    store, and every CTA waits for all slots (acquire loads) and adds them in
+//    store, and every CTA waits for all slots (one warp polls them with relaxed
+//    loads, then an acquire fence) and adds them in
 //    the fixed order of reduce256.  A slot holds a signalling NaN until its sum
 //    arrives -- no arithmetic result has those bits -- so the data carries the
 //    barrier: no arrival counter and no second round trip.  Three slot buffers
@@ -44,7 +45,7 @@ namespace {
 // returns a signalling NaN.
 constexpr uint64_t kSlotEmpty = 0x7FF0DEADBEEF0001ull;
 constexpr int kResMaxWidth = 8;  // nonzeros of the longest row
-constexpr int kResMaxSlotsPerThread = 4;  // row blocks <= 1024
+constexpr int kResMaxSlots = 1024;  // row blocks: 32 per polling lane
 
 struct ResArgs {
     const int32_t* row_ptr;
@@ -67,11 +68,6 @@ __device__ __forceinline__ void st_release(double* p, double v) {
 }
 __device__ __forceinline__ void st_relaxed_bits(double* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ uint64_t ld_acquire_bits(const double* p) {
-    uint64_t v;
-    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
 }
 
 __global__ void fill_slots_kernel(double* slots, int64_t count) {
@@ -103,37 +99,52 @@ __device__ __forceinline__ void publish(const double (&d)[B], double (*scr)[kWar
     }
 }
 
+__device__ __forceinline__ uint64_t ld_relaxed_bits(const double* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Waits for every slot of `cur` and returns their total in reduce256's order
-// (every thread gets it).  Returns false in every thread when a wait gave up.
+// (every thread gets it).  One warp polls -- lane l the slots l, l + 32, ...,
+// with relaxed loads, the outstanding ones re-read together -- and, once all
+// have arrived, a fence gives it acquire order; the CTA then reads the sums
+// and adds them in the fixed order.  Returns false in every thread when the
+// wait gave up.
 __device__ __forceinline__ bool gather_total(const double* cur, int nblk, double* red,
-                                             double* bc, unsigned int* err, double* out) {
+                                             double* bc, unsigned int* err, double* out,
+                                             bool* okf) {
     const int t = threadIdx.x;
-    uint64_t v[kResMaxSlotsPerThread];
-    const int m = t < nblk ? (nblk - 1 - t) / kThreads + 1 : 0;
-    unsigned pending = (1u << m) - 1u;
-    bool ok = true;
-    const uint64_t t0 = global_timer_ns();
-    for (uint32_t it = 0; pending; ++it) {
+    if (t < 32) {
+        bool ok = true;
+        uint32_t pending = 0;
+        for (int j = 0; j < 32; ++j)
+            if (t + 32 * j < nblk) pending |= 1u << j;
+        const uint64_t t0 = global_timer_ns();
+        for (uint32_t it = 0; pending; ++it) {
+            uint64_t v[32];
 #pragma unroll
-        for (int j = 0; j < kResMaxSlotsPerThread; ++j)
-            if (pending & (1u << j)) v[j] = ld_acquire_bits(cur + t + j * kThreads);
+            for (int j = 0; j < 32; ++j)
+                if (pending & (1u << j)) v[j] = ld_relaxed_bits(cur + t + 32 * j);
 #pragma unroll
-        for (int j = 0; j < kResMaxSlotsPerThread; ++j)
-            if ((pending & (1u << j)) && v[j] != kSlotEmpty) pending &= ~(1u << j);
-        if (pending && (it & 63u) == 63u &&
-            (global_timer_ns() - t0 > kWaitLimitNs || it > (1u << 28))) {
-            atomicOr(err, kErrWaitTimeout);
-            ok = false;
-            break;
+            for (int j = 0; j < 32; ++j)
+                if ((pending & (1u << j)) && v[j] != kSlotEmpty) pending &= ~(1u << j);
+            if (pending && (it & 63u) == 63u &&
+                (global_timer_ns() - t0 > kWaitLimitNs || it > (1u << 28))) {
+                atomicOr(err, kErrWaitTimeout);
+                ok = false;
+                break;
+            }
         }
+        __threadfence();  // acquire: the publishers' writes before their release stores
+        const bool all = __all_sync(0xffffffffu, ok);
+        if (t == 0) *okf = all;
     }
+    __syncthreads();
+    const bool all_ok = *okf;
     double s = 0.0;
-    if (ok) {
-#pragma unroll
-        for (int j = 0; j < kResMaxSlotsPerThread; ++j)
-            if (j < m) s += __longlong_as_double(static_cast<long long>(v[j]));
-    }
-    const bool all_ok = __syncthreads_and(ok) != 0;
+    if (all_ok && t < kThreads)
+        for (int i = t; i < nblk; i += kThreads) s += __ldcg(cur + i);
     const double tot = block_sum8(s, red);
     if (t == 0) *bc = tot;
     __syncthreads();
@@ -151,6 +162,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
     __shared__ double scr[B][kWarps];
     __shared__ double red[kWarps + 1];
     __shared__ double bc;
+    __shared__ bool okf;
     const int t = threadIdx.x;
     CgState* st = a.st;
     if (__ldcg(&st->done)) return;  // the initial kernel decided already
@@ -222,7 +234,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
         double* nxt = a.slots + ((phase + 1) % 3) * a.nblk;
         publish<B>(d, scr, nown, blk0, cur, nxt);
         double pAp;
-        if (!gather_total(cur, a.nblk, red, &bc, a.err, &pAp)) {
+        if (!gather_total(cur, a.nblk, red, &bc, a.err, &pAp, &okf)) {
             failed = true;
             break;
         }
@@ -256,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
         nxt = a.slots + ((phase + 1) % 3) * a.nblk;
         publish<B>(s, scr, nown, blk0, cur, nxt);
         double rr_new;
-        if (!gather_total(cur, a.nblk, red, &bc, a.err, &rr_new)) {
+        if (!gather_total(cur, a.nblk, red, &bc, a.err, &rr_new, &okf)) {
             failed = true;
             break;
         }
@@ -337,7 +349,7 @@ int plan_resident(const nm_csr* A, CgWorkspace* ws) {
         W = std::max(W, len);
     }
     const int64_t nblk = (n + kThreads - 1) / kThreads;
-    if (A->nblk != nblk || nblk > int64_t(kResMaxSlotsPerThread) * kThreads) return NM_OK;
+    if (A->nblk != nblk || nblk > kResMaxSlots) return NM_OK;
     const int sms = sm_count();
     const int B = static_cast<int>((nblk + sms - 1) / sms);
     if (B < 1 || B > kResidentMaxTiles) return NM_OK;

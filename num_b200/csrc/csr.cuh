@@ -142,7 +142,7 @@ int rebuild_blocks(nm_csr* A);
 // Longest row the warp-gather kernel takes (each row is summed by one lane).
 constexpr int32_t kWarpGatherMaxRow = 4096;
 // Rows sorted by length together in the gather kernel's sliced copy.
-constexpr int32_t kSellWindow = 1024;
+constexpr int32_t kSellWindow = 65536;
 // Builds A's sliced copy for the gather kernel once (spmv.cu); NM_OK also
 // when the layout would pad too much (A->sell_ready stays false).
 int build_sell(nm_csr* A);
