@@ -107,13 +107,14 @@ __device__ __forceinline__ uint64_t ld_relaxed_bits(const double* p) {
 
 // Waits for every slot of `cur` and returns their total in reduce256's order
 // (every thread gets it).  One warp polls -- lane l the slots l, l + 32, ...,
-// with relaxed loads, the outstanding ones re-read together -- and, once all
-// have arrived, a fence gives it acquire order; the CTA then reads the sums
-// and adds them in the fixed order.  Returns false in every thread when the
+// with relaxed loads, the outstanding ones re-read together, each sum parked
+// in shared memory as it arrives -- and, once all have, a fence gives it
+// acquire order; the CTA then adds the parked sums in the fixed order.
+// Returns false in every thread when the
 // wait gave up.
 __device__ __forceinline__ bool gather_total(const double* cur, int nblk, double* red,
                                              double* bc, unsigned int* err, double* out,
-                                             bool* okf) {
+                                             bool* okf, double* sv) {
     const int t = threadIdx.x;
     if (t < 32) {
         bool ok = true;
@@ -128,7 +129,10 @@ __device__ __forceinline__ bool gather_total(const double* cur, int nblk, double
                 if (pending & (1u << j)) v[j] = ld_relaxed_bits(cur + t + 32 * j);
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-                if ((pending & (1u << j)) && v[j] != kSlotEmpty) pending &= ~(1u << j);
+                if ((pending & (1u << j)) && v[j] != kSlotEmpty) {
+                    pending &= ~(1u << j);
+                    sv[t + 32 * j] = __longlong_as_double(static_cast<long long>(v[j]));
+                }
             if (pending && (it & 63u) == 63u &&
                 (global_timer_ns() - t0 > kWaitLimitNs || it > (1u << 28))) {
                 atomicOr(err, kErrWaitTimeout);
@@ -144,7 +148,7 @@ __device__ __forceinline__ bool gather_total(const double* cur, int nblk, double
     const bool all_ok = *okf;
     double s = 0.0;
     if (all_ok && t < kThreads)
-        for (int i = t; i < nblk; i += kThreads) s += __ldcg(cur + i);
+        for (int i = t; i < nblk; i += kThreads) s += sv[i];
     const double tot = block_sum8(s, red);
     if (t == 0) *bc = tot;
     __syncthreads();
@@ -163,6 +167,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
     __shared__ double red[kWarps + 1];
     __shared__ double bc;
     __shared__ bool okf;
+    __shared__ double sv[kResMaxSlots];  // the sums of the phase, as the polling warp saw them
     const int t = threadIdx.x;
     CgState* st = a.st;
     if (__ldcg(&st->done)) return;  // the initial kernel decided already
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
         double* nxt = a.slots + ((phase + 1) % 3) * a.nblk;
         publish<B>(d, scr, nown, blk0, cur, nxt);
         double pAp;
-        if (!gather_total(cur, a.nblk, red, &bc, a.err, &pAp, &okf)) {
+        if (!gather_total(cur, a.nblk, red, &bc, a.err, &pAp, &okf, sv)) {
             failed = true;
             break;
         }
@@ -268,7 +273,7 @@ __global__ void __launch_bounds__(kThreads) cg_resident_kernel(ResArgs a) {
         nxt = a.slots + ((phase + 1) % 3) * a.nblk;
         publish<B>(s, scr, nown, blk0, cur, nxt);
         double rr_new;
-        if (!gather_total(cur, a.nblk, red, &bc, a.err, &rr_new, &okf)) {
+        if (!gather_total(cur, a.nblk, red, &bc, a.err, &rr_new, &okf, sv)) {
             failed = true;
             break;
         }
