@@ -1338,7 +1338,7 @@ def main():
     ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2],
                     help="nm_cg_set_persistent: 1 resident / persistent (default), 2 the "
                          "TMA-pipelined persistent solve only, 0 CUDA-graph chunks")
-    ap.add_argument("--engine-mode", default="persistent", choices=["persistent", "graph"],
+    ap.add_argument("--engine-mode", default="graph", choices=["persistent", "graph"],
                     help="nm_solver_set_persistent: one cooperative launch per engine step, or "
                          "a CUDA graph of kernels")
     args = ap.parse_args()

@@ -57,11 +57,16 @@ typedef struct {
 
 /* nm_tuning.kernel.  BLOCKS: the row-block TMA pipeline.  GATHER: one warp per
  * 32 rows streaming the nonzeros and gathering x through L2, every row summed
- * serially in CSR order (for scattered columns).  AUTO: GATHER when at least
- * 3/4 of the nonzeros lie in row blocks without x windows and no row has more
- * than 4096 nonzeros, else BLOCKS.  CG and the batched engine always use the
+ * serially in CSR order (for scattered columns).  SLICED: the same serial row
+ * sums from a copy of the matrix sorted by row length and stored as
+ * column-major 32-row slices, lane per row (built when first selected; a
+ * matrix it would pad to more than twice its nonzeros runs GATHER instead).
+ * AUTO: GATHER when at least 3/4 of the nonzeros lie in row blocks without x
+ * windows and no row has more than 4096 nonzeros, else BLOCKS.  The
+ * autotuner times all three.  CG and the batched engine always use the
  * row-block pipeline. */
-enum nm_kernel { NM_KERNEL_AUTO = 1, NM_KERNEL_BLOCKS = 2, NM_KERNEL_GATHER = 3 };
+enum nm_kernel { NM_KERNEL_AUTO = 1, NM_KERNEL_BLOCKS = 2, NM_KERNEL_GATHER = 3,
+                 NM_KERNEL_SLICED = 4 };
 
 typedef struct nm_csr nm_csr;    /* device CSR matrix (CrsMatrixHandle)   */
 typedef struct nm_dist nm_dist;  /* one rank's slice (DistCrsHandle)      */
@@ -157,7 +162,7 @@ int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t);
 int nm_csr_get_tuning(const nm_csr* A, nm_tuning* t);
 
 /* The plain-SpMV kernel nm_spmv runs on A under its tuning (AUTO resolved):
- * NM_KERNEL_BLOCKS or NM_KERNEL_GATHER. */
+ * NM_KERNEL_BLOCKS, NM_KERNEL_GATHER or NM_KERNEL_SLICED. */
 int nm_csr_spmv_kernel(const nm_csr* A, int32_t* kernel);
 
 /* One timed candidate of nm_csr_autotune. */
@@ -287,12 +292,12 @@ typedef struct {
                            solve's estimate (default 2; <= 0 keeps the default) */
 } nm_solver_opts;
 
-/* Process-wide choice of how a step's inner iterations run: 1 (default) one
- * persistent cooperative launch per step (SpMV, update and p update of every
- * live system separated by grid barriers, ending as soon as no system
- * iterates), when the device supports it; 0 a CUDA graph whose loop body
- * launches those phases as kernels.  Both give the same bits.  Other values:
- * NM_ERR_INVALID. */
+/* Process-wide choice of how a step's inner iterations run: 0 (default) a
+ * CUDA graph whose loop body launches the SpMV, update and p update of every
+ * live system as kernels; 1 one persistent cooperative launch per step (the
+ * same phases separated by grid barriers, ending as soon as no system
+ * iterates), when the device supports it.  Both give the same bits.  Other
+ * values: NM_ERR_INVALID. */
 int nm_solver_set_persistent(int32_t enable);
 
 /* A solver with a device arena for up to max_rows rows and max_nnz nonzeros

@@ -252,7 +252,7 @@ struct CoopFormPApEpi {
 // r0) = r0 = p0.  Same iterates as the three-barrier form, one grid barrier
 // fewer per iteration, at the cost of a second set of staged windows.
 template <int TILE, int STAGES, bool FORMED>
-__global__ void __launch_bounds__(kCtaThreads)
+__global__ void __launch_bounds__(kCtaThreads, 2)
     cg_coop_kernel(CsrView<double> M, CgState* st, double* p, double* p2, double* Ap, double* r,
                    double* part_a, double* part_b, int grid_vec, int64_t n, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -520,9 +520,9 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
         // than the SpMV grid has.  The two-barrier form stages twice the
         // windows, so fewer of its CTAs fit an SM; where the grid does not fit
         // it, the three-barrier form runs.
-        ws->coop = coop_ok && int64_t(occ_c) * sm_count() >= ws->grid_spmv &&
-                   n <= kCoopMaxRows;
-        ws->coop_formed = ws->coop && int64_t(occ_f) * sm_count() >= ws->grid_spmv;
+        const bool fits = coop_ok && n <= kCoopMaxRows;
+        ws->coop_formed = fits && int64_t(occ_f) * sm_count() >= ws->grid_spmv;
+        ws->coop = ws->coop_formed || (fits && int64_t(occ_c) * sm_count() >= ws->grid_spmv);
         if (coop_ok) {
             st = plan_resident(A, ws.get());
             if (st != NM_OK) return st;

@@ -117,9 +117,9 @@ int normalise_tuning(nm_tuning& t) {
     if (t.grid_mult < 0) t.grid_mult = 0;
     if (t.stages <= 0) t.stages = kDefaultStages;
     if (t.kernel <= 0) t.kernel = NM_KERNEL_AUTO;
-    if (t.kernel > NM_KERNEL_GATHER)
-        return fail(NM_ERR_INVALID, "tuning: kernel must be 1 (auto), 2 (blocks) or 3 (gather) "
-                    "(got %d)", t.kernel);
+    if (t.kernel > NM_KERNEL_SLICED)
+        return fail(NM_ERR_INVALID, "tuning: kernel must be 1 (auto), 2 (blocks), 3 (gather) or "
+                    "4 (sliced) (got %d)", t.kernel);
     if (t.stages < 2 || t.stages > 4)
         return fail(NM_ERR_INVALID, "tuning: stages must be 2, 3 or 4 (got %d)", t.stages);
     if (t.tile != 1024 && t.tile != 2048 && t.tile != 4096)
@@ -220,9 +220,10 @@ int rebuild_blocks(nm_csr* A) {
         const bool scattered = A->nnz > 0 && 4 * gathered >= 3 * int64_t(A->nnz) &&
                                max_row <= kWarpGatherMaxRow;
         A->warp_gather = A->tune.kernel == NM_KERNEL_GATHER ||
+                         A->tune.kernel == NM_KERNEL_SLICED ||
                          (A->tune.kernel == NM_KERNEL_AUTO && scattered);
     }
-    if (A->warp_gather && !A->sell_tried) {
+    if (A->tune.kernel == NM_KERNEL_SLICED && !A->sell_tried) {
         const int st = build_sell(A);
         if (st != NM_OK) return st;
     }
@@ -489,7 +490,9 @@ extern "C" int nm_csr_set_tuning(nm_csr* A, const nm_tuning* t) {
 extern "C" int nm_csr_spmv_kernel(const nm_csr* A, int32_t* kernel) {
     nm::clear_error();
     if (!A || !kernel) return fail(NM_ERR_INVALID, "nm_csr_spmv_kernel: NULL argument");
-    *kernel = A->warp_gather ? NM_KERNEL_GATHER : NM_KERNEL_BLOCKS;
+    *kernel = !A->warp_gather ? NM_KERNEL_BLOCKS
+              : (A->tune.kernel == NM_KERNEL_SLICED && A->sell_ready ? NM_KERNEL_SLICED
+                                                                      : NM_KERNEL_GATHER);
     return NM_OK;
 }
 

@@ -393,7 +393,9 @@ static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
 template <typename V, typename X, typename A>
 static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     if (Am->warp_gather)
-        return Am->sell_ready ? launch_sell<V, X, A>(Am, x, y, s) : launch_gather<V, X, A>(Am, x, y, s);
+        return Am->tune.kernel == NM_KERNEL_SLICED && Am->sell_ready
+                   ? launch_sell<V, X, A>(Am, x, y, s)
+                   : launch_gather<V, X, A>(Am, x, y, s);
     switch (Am->tune.tile) {
         case 1024: return launch_stages<V, X, A, 1024>(Am, x, y, s);
         case 2048: return launch_stages<V, X, A, 2048>(Am, x, y, s);
@@ -532,7 +534,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // One warp per row (k wide enough for the row's columns to span the warp),
-// each CTA over its own contiguous range of rows.  The warp reads a row's first
+// rows strided by the number of resident warps.  The warp reads a row's first
 // 32 columns and values in one coalesced access, one row ahead, and its
 // row_ptr entries two rows ahead, so the row's X loads are the only memory
 // latency on its critical path; later 32-nonzero windows of longer rows are
@@ -550,14 +552,15 @@ __global__ void __launch_bounds__(kBatchWarpThreads)
                            const double* __restrict__ X, double* __restrict__ Y) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    // CTA b owns the contiguous rows [r_beg, r_end) and its warps take them in
-    // turn, so the X rows that neighbouring rows share (the band of the
-    // matrix) are read by one SM close together in time and reused from L1.
-    const int64_t per = (int64_t(nrows) + gridDim.x - 1) / gridDim.x;
-    const int64_t r_beg = int64_t(blockIdx.x) * per;
-    const int64_t r_end = r_beg + per < nrows ? r_beg + per : nrows;
-    const int64_t nw = kBatchWarpThreads / 32;
-    int64_t row = r_beg + (threadIdx.x >> 5);  // same for the warp
+    // Rows strided over all resident warps: the whole GPU sweeps the rows in
+    // order, so the X rows a band of rows shares (the +-1, +-L and +-L^2
+    // neighbours of a stencil) are read close together in time and stay in
+    // L2 between their uses.  (A contiguous row range per CTA, for L1 reuse of
+    // the +-1 neighbours, measured 1,025 us against 663 us on the 100^3
+    // Laplacian with k = 128: the CTAs' separate sweeps overflow L2.)
+    const int64_t r_end = nrows;
+    const int64_t nw = int64_t(gridDim.x) * (kBatchWarpThreads / 32);
+    int64_t row = (int64_t(blockIdx.x) * kBatchWarpThreads + threadIdx.x) >> 5;  // same for the warp
     if (row >= r_end) return;
     int32_t s0 = __ldg(rp + row), s1 = __ldg(rp + row + 1);
     int32_t c_nx = 0;

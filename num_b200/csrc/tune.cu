@@ -6,7 +6,8 @@
 //   short_max 32, 64             rows up to this length are thread-per-row
 //   stages    2, 3, 4            TMA ring depth (skipped when it does not fit)
 //   grid_mult 0 (all resident CTAs), 1, 2 CTAs per SM
-//   and, once, the warp-gather kernel (which ignores the four above)
+//   and, once each, the warp-gather and sliced gather kernels (which ignore
+//   the four above)
 // max_rows stays at its default (one consumer thread per row of a block).
 // tile and short_max change the descriptors (a host rebuild per pair);
 // stages and grid_mult only change the launch.  short_max never goes below
@@ -114,11 +115,15 @@ extern "C" int nm_csr_autotune(nm_csr* A, const void* x, void* y, void* stream,
                 }
             if (st != NM_OK) break;
         }
-    if (st == NM_OK) {
+    for (const int kern : {int(NM_KERNEL_GATHER), int(NM_KERNEL_SLICED)}) {
+        if (st != NM_OK) break;
         nm_tuning t = start;
-        t.kernel = NM_KERNEL_GATHER;
+        t.kernel = kern;
         A->tune = t;
         st = rebuild_blocks(A);
+        // a matrix whose sliced copy would pad too much runs the gather kernel
+        // under NM_KERNEL_SLICED: nothing new to time
+        if (st == NM_OK && kern == NM_KERNEL_SLICED && !A->sell_ready) break;
         float us = 0.f;
         if (st == NM_OK) st = time_spmv(A, x, y, s, 1, reps, ev.a, ev.b, &us);
         if (st == NM_OK) {

@@ -41,7 +41,7 @@ __all__ = [
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
 # nm_tuning.kernel: the plain SpMV kernel (auto, the row-block pipeline, the warp gather)
-_KERNELS = {"auto": 1, "blocks": 2, "gather": 3}
+_KERNELS = {"auto": 1, "blocks": 2, "gather": 3, "sliced": 4}
 
 
 def _dist():

@@ -195,7 +195,7 @@ def test_tune_kernel_names_checked_on_host(nmlib):
     from num_b200 import kokkos_spmv as k
     with pytest.raises(ValueError, match="kernel must be one of"):
         k.tune(None, kernel="fastest")
-    assert k._KERNELS == {"auto": 1, "blocks": 2, "gather": 3}
+    assert k._KERNELS == {"auto": 1, "blocks": 2, "gather": 3, "sliced": 4}
     t = C.c_int32()
     st = nmlib.nm_csr_spmv_kernel(None, C.byref(t))
     from num_b200 import _lib

@@ -265,13 +265,13 @@ def test_persistent_step_equals_graph_step(kspmv, nmlib, precision):
     systems.insert(7, (L, rng.standard_normal(L.nrows)))
     out = []
     try:
-        for mode in (1, 0, 1):
+        for mode in (0, 1, 0):
             nmlib.nm_solver_set_persistent(mode)
             S = _solver(precision, rows=1_000_000, nnz=6_000_000, systems=64)
             out.append(S.solve(systems, tol=1e-9, max_iter=20000, chunk=16))
             del S
     finally:
-        nmlib.nm_solver_set_persistent(1)
+        nmlib.nm_solver_set_persistent(0)
     for run in out[1:]:
         for (xa, ia), (xb, ib) in zip(out[0], run):
             assert ia == ib and np.array_equal(xa, xb)

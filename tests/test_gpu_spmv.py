@@ -169,6 +169,35 @@ def test_gather_fp32_and_bf16_every_row_bit_exact(kspmv, oracle):
     assert np.array_equal(yb, oracle.spmv(A.row_ptr, A.col_idx, vb, x))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+@pytest.mark.parametrize("case", ["power_law", "random_sparse", "ragged"])
+def test_sliced_kernel_every_row_bit_exact(kspmv, oracle, precision, case):
+    # The sliced gather kernel (rows sorted by length, column-major 32-row
+    # slices, lane per row) sums every row serially in CSR order: bit-identical
+    # to the serial oracle for rows of any length, in every precision; empty
+    # rows give 0 and the permuted rows land in their own places.
+    if case == "power_law":
+        A = gen.power_law(150_000, seed=17)
+        x = np.random.default_rng(17).uniform(-1, 1, A.ncols)
+    elif case == "random_sparse":
+        A = gen.get_matrix("random_sparse", 30_000)
+        x = np.random.default_rng(18).uniform(-1, 1, A.ncols)
+    else:
+        A, rng = _scattered(70_001, [0, 1, 3, 9, 40, 200], 19, ncols=300_000)
+        x = rng.uniform(-1, 1, A.ncols)
+    vals = A.values
+    if precision == "fp32":
+        vals, x = A.values.astype(np.float32), x.astype(np.float32)
+    elif precision == "bf16":
+        from num_b200.kokkos_spmv import _values_for
+        bits, _ = _values_for(A.values, "bf16")
+        vals, x = (bits.astype(np.uint32) << 16).view(np.float32), x.astype(np.float32)
+    y, M = _run(kspmv, A, x, precision=precision, tuning={"kernel": "sliced"})
+    assert kspmv.spmv_kernel(M) == "sliced"
+    assert np.array_equal(y, oracle.spmv(A.row_ptr, A.col_idx, vals, x))
+    assert np.all(y[np.diff(A.row_ptr) == 0] == 0.0)
+
+
 def test_tune_kernel_argument_errors(kspmv):
     A = gen.tridiag4()
     M = kspmv.upload_csr(*A.astuple())
@@ -336,7 +365,8 @@ def test_autotune_installs_a_valid_tuning(kspmv, oracle, tmp_path, monkeypatch):
     assert res["tile"] in (1024, 2048, 4096) and res["short_max"] in (32, 64)
     assert res["stages"] in (2, 3, 4) and res["grid_mult"] in (0, 1, 2)
     assert res["us"] == min(t["us"] for t in res["trials"])
-    assert {t["kernel"] for t in res["trials"]} == {"blocks", "gather"}
+    assert {"blocks", "gather"} <= {t["kernel"] for t in res["trials"]} <= \
+        {"blocks", "gather", "sliced"}
     assert {k: res[k] for k in ("tile", "short_max", "stages", "grid_mult", "kernel")} == \
         {k: kspmv.tuning(M)[k] for k in ("tile", "short_max", "stages", "grid_mult", "kernel")}
     xt = torch.tensor(x, device="cuda")
