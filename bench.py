@@ -1335,9 +1335,10 @@ def main():
                     help="serve_c5: the engine's preconditioner")
     ap.add_argument("--no-plain", action="store_true",
                     help="serve_c5: skip the plain FP64 drop-in comparison")
-    ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2],
-                    help="nm_cg_set_persistent: 1 resident / persistent (default), 2 the "
-                         "TMA-pipelined persistent solve only, 0 CUDA-graph chunks")
+    ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="nm_cg_set_persistent: 1 persistent (default), 2 the TMA-pipelined "
+                         "persistent solve only, 3 the resident solve only, 0 CUDA-graph "
+                         "chunks")
     ap.add_argument("--engine-mode", default="graph", choices=["persistent", "graph"],
                     help="nm_solver_set_persistent: one cooperative launch per engine step, or "
                          "a CUDA graph of kernels")

@@ -225,11 +225,11 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
 /* ---- CG -------------------------------------------------------------------- */
 
 /* Process-wide choice of how nm_cg_local / nm_dist_cg_single iterate:
- * 1 (default) one persistent cooperative launch per solve when the device
- * supports it and the matrix's SpMV grid is co-resident -- the resident solve
- * (matrix rows and vectors kept on chip, two grid-wide sums per iteration)
- * for systems of at most 262,144 rows of at most 8 nonzeros each, else the
- * persistent TMA-pipelined solve; 2 the persistent TMA-pipelined solve only;
+ * 1 (default) one persistent cooperative launch per solve for systems of at
+ * most 262,144 rows -- the TMA-pipelined persistent solve where its SpMV grid
+ * is co-resident, else the resident solve (matrix rows and vectors kept on
+ * chip, two grid-wide sums per iteration; rows of at most 8 nonzeros);
+ * 2 the TMA-pipelined persistent solve only; 3 the resident solve only;
  * 0 CUDA-graph chunks of three kernels per iteration.  All give the same
  * iterates, bit for bit (every dot product is summed in one fixed order: per
  * row block or 256-row tile, then over the blocks).  Other values:

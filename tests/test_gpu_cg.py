@@ -298,7 +298,7 @@ def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
     out = []
     try:
-        for persistent in (1, 0, 2, 1):
+        for persistent in (1, 0, 2, 3, 1):
             nmlib.nm_cg_set_persistent(persistent)
             x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
             info = kspmv.cg_solve_local(M, b, x, tol=1e-9, max_iter=3000)
