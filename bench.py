@@ -72,6 +72,12 @@ WORKLOADS = {
                       "FP64", "batch", "fp64"),
     "cg_c1": ("2-D 5-point Laplacian 256^2, plain FP64 CG, b = A*1, x0 = 0, tol 1e-8", "cg",
               "fp64"),
+    "cg_1m": ("2-D 5-point Laplacian 1024^2 (1,048,576 rows: the CUDA-graph path), plain FP64 "
+              "CG, b = A*1, x0 = 0, tol 1e-8", "cg", "fp64"),
+    "vec_c2a": ("CG vector ops at 4,096,000 elements: axpy, axpy2 and dot per step", "vec",
+                "fp64"),
+    "halo_c2a": ("halo pack + unpack of the 160^3 Laplacian split into 8 row slabs (8 virtual "
+                 "ranks on one GPU)", "halo", "fp64"),
     "cg_c4_fp64": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG FP64 to 1e-10",
                    "engine", "fp64"),
     "cg_c4_fp32": ("3-D variable-coefficient Poisson 128^3 (seed 3), Jacobi PCG FP32 + FP64 "
@@ -137,6 +143,9 @@ def make_workload(name):
         seed = 1
     elif name in ("spmv_c1", "cg_c1"):
         A = gen.laplacian_2d(256)
+        seed = 0
+    elif name == "cg_1m":
+        A = gen.laplacian_2d(1024)
         seed = 0
     elif name.startswith("spmv_c3"):
         mats, xs = gen.banded_batch(4096, seed=2)
@@ -664,13 +673,13 @@ def cpu_baseline_batch(A, k, budget_s=10.0):
 
 # ---- our arm: plain CG (the drop-in cg_solve_local) ------------------------------------
 
-def cg_c1_measure(dev, steps, warmup, with_clock=True, local_rank=0):
+def cg_c1_measure(dev, steps, warmup, with_clock=True, local_rank=0, name="cg_c1"):
     """Device-timed plain FP64 CG solves (b = A 1 resident, x zeroed on the
     device each step) and the same through the public API with host copies."""
     import torch
 
     from num_b200 import kokkos_spmv as kspmv
-    A, _ = make_workload("cg_c1")
+    A, _ = make_workload(name)
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
     bh = A.to_scipy() @ np.ones(A.ncols)
     b = torch.tensor(bh, device=dev)
@@ -737,7 +746,7 @@ def run_cg(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     desc, _, precision = WORKLOADS[args.workload]
     barrier(world)
-    r = cg_c1_measure(dev, args.steps, args.warmup, local_rank=local_rank)
+    r = cg_c1_measure(dev, args.steps, args.warmup, local_rank=local_rank, name=args.workload)
     barrier(world)
     ms, e2e_ms = max_over_ranks([r["ms"], r["e2e_ms"]], world, dev)
     if rank != 0:
@@ -751,8 +760,8 @@ def run_cg(args, rank, world, local_rank):
     config = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
               "tol": 1e-8, "iters_per_solve": it_per_solve,
               "final_residual": r["info"]["residual"], "max_abs_err_vs_ones": r["max_err_vs_ones"],
-              "l2": "operands fit L2 (11.5 MB): L2 flushed before every solve, solves timed "
-                    "alone; within a solve the iterations are L2-resident and latency-bound",
+              "l2": "operands fit L2 (%.1f MB): L2 flushed before every solve, solves timed "
+                    "alone; within a solve the iterations run from L2" % (per_it / 1e6),
               "parallelism": f"replicas x{world}",
               "api": "kokkos_spmv.cg_solve_local (C ABI nm_cg_local)",
               "path": r["path"], "cg_mode": args.cg_mode}
@@ -1273,7 +1282,7 @@ def run_reference(args, rank, world):
     elif kind in ("cg", "engine"):
         from num_b200 import generators as gen
         if kind == "cg":
-            A, _ = make_workload("cg_c1")
+            A, _ = make_workload(args.workload)
             b, tol, pre, iters = A.to_scipy() @ np.ones(A.ncols), 1e-8, False, None
         else:
             A, b = gen.varcoef_poisson_3d(128, seed=3)
@@ -1284,6 +1293,44 @@ def run_reference(args, rank, world):
         val, unit, sample = cb["value"], "solves/s", cb["sample"] + f" ({note})"
         cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz}
         ms_step = 1e3 / val
+    elif kind == "vec":
+        from oracle import oracle
+        n = VEC_N
+        rng = np.random.default_rng(5)
+        x, y = rng.random(n), rng.random(n)
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < min(30.0, 1.0 * (args.steps + args.warmup)):
+            z = oracle.axpy(0.5, x, y)
+            w = oracle.axpy2(0.25, x, -0.5, z)
+            oracle.dot(x, w)
+            reps += 1
+        el = (time.perf_counter() - t0) / reps
+        val, unit = vec_bytes(n) / el / 1e9, "GB/s"
+        sample = (f"{reps} steps of axpy + axpy2 + dot on {n} doubles, oracle/oracle.c "
+                  f"(serial loops) ({note})")
+        cfg = {"workload": desc, "name": args.workload, "n": n, "bytes_per_step": vec_bytes(n)}
+        ms_step = el * 1e3
+    elif kind == "halo":
+        from oracle import oracle
+        A, parts = halo_workload()
+        x = np.random.default_rng(6).uniform(-1, 1, A.ncols)
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < min(30.0, 1.0 * (args.steps + args.warmup)):
+            for p in parts:
+                buf = oracle.halo_pack(p["send_idx"], x[p["row_start"]:p["row_end"]])
+                ext = np.empty(p["local_n"] + p["n_ghost"])
+                ext[p["local_n"]:] = x[p["ghost_ids"]]  # unpack of the received ghosts
+                del buf, ext
+            reps += 1
+        el = (time.perf_counter() - t0) / reps
+        nbytes = sum(halo_bytes(p["total_send"], p["n_ghost"]) for p in parts)
+        val, unit = nbytes / el / 1e9, "GB/s"
+        sample = f"{reps} steps over {len(parts)} slabs, oracle.halo_pack + numpy scatter ({note})"
+        cfg = {"workload": desc, "name": args.workload, "ranks": len(parts),
+               "bytes_per_step": nbytes}
+        ms_step = el * 1e3
     else:  # serve
         from num_b200 import serve
         requests = serve.make_requests(args.requests, rate=args.rate, seed=4, pool=args.pool)
@@ -1305,7 +1352,205 @@ def run_reference(args, rank, world):
     }
 
 
-DEFAULT_STEPS = {"spmv": 2000, "batch": 100, "cg": 50, "engine": 5, "serve": 3}
+# ---- CG vector ops and halo pack / unpack (their own kernels, measured alone) ----------
+
+VEC_N = 4_096_000  # the 160^3 system's length
+
+
+def vec_bytes(n):
+    """axpy (x, y read, z written) + axpy2 (same) + dot (x, y read)."""
+    return 24 * n + 24 * n + 16 * n
+
+
+def halo_bytes(total_send, n_ghost):
+    """pack: index, gathered x entry, buffer entry per sent value; unpack:
+    buffer entry read, ghost slot written."""
+    return total_send * (4 + 8 + 8) + n_ghost * 16
+
+
+def halo_workload(P=8):
+    """The 160^3 Laplacian's halo plan for P row slabs (the library's host-only
+    planner, nm_dist_plan): per rank its row range, send index list (local)
+    and ghost ids."""
+    from num_b200 import _lib
+    from num_b200 import generators as gen
+    lib = _lib.load()
+    A = gen.laplacian_3d(160)
+    rp, ci, v = (np.ascontiguousarray(a) for a in (A.row_ptr, A.col_idx, A.values))
+    parts = []
+    for r in range(P):
+        h = C.c_void_p()
+        _lib.check(lib.nm_dist_plan(rp.ctypes.data, ci.ctypes.data, v.ctypes.data, A.nrows,
+                                    A.ncols, r, P, C.byref(h)), "nm_dist_plan")
+        info = [C.c_int32() for _ in range(7)]
+        _lib.check(lib.nm_dist_info(h, *[C.byref(i) for i in info]), "nm_dist_info")
+        gn, rs, re, ng, ts, nsn, nrn = (i.value for i in info)
+        send_idx = np.empty(max(ts, 1), np.int32)
+        ghost_ids = np.empty(max(ng, 1), np.int32)
+        a1, a2, a3 = (np.empty(max(nsn, 1), np.int32) for _ in range(3))
+        _lib.check(lib.nm_dist_send_plan(h, a1.ctypes.data, a2.ctypes.data, a3.ctypes.data,
+                                         send_idx.ctypes.data), "send plan")
+        b1, b2, b3 = (np.empty(max(nrn, 1), np.int32) for _ in range(3))
+        _lib.check(lib.nm_dist_recv_plan(h, b1.ctypes.data, b2.ctypes.data, b3.ctypes.data,
+                                         ghost_ids.ctypes.data), "recv plan")
+        lib.nm_dist_destroy(h)
+        parts.append({"row_start": rs, "row_end": re, "local_n": re - rs, "n_ghost": ng,
+                      "total_send": ts, "send_idx": send_idx[:ts], "ghost_ids": ghost_ids[:ng]})
+    return A, parts
+
+
+def time_ops(ops, stream, steps, warmup):
+    """Each op of `ops` (name -> callable enqueueing one kernel) timed with
+    its own CUDA events over `steps` rounds after `warmup` rounds; returns
+    (ms of the whole timed region, {name: average ms})."""
+    import torch
+    for _ in range(warmup):
+        for f in ops.values():
+            f()
+    torch.cuda.synchronize()
+    ev = {k: [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)] for k in ops}
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(steps):
+        for k, f in ops.items():
+            ev[k][i][0].record(stream)
+            f()
+            ev[k][i][1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    avg = {k: sum(a.elapsed_time(b) for a, b in v) / steps for k, v in ev.items()}
+    return t0.elapsed_time(t1), avg
+
+
+def run_vec(args, rank, world, local_rank):
+    import torch
+
+    from num_b200 import _lib
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    n = VEC_N
+    g = torch.Generator(device=dev).manual_seed(5)
+    x = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    y = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    z, w = torch.empty_like(x), torch.empty_like(x)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    res = C.c_double()
+    ops = {
+        "axpy": lambda: lib.nm_axpy(n, 0.5, x.data_ptr(), y.data_ptr(), z.data_ptr(), s),
+        "axpy2": lambda: lib.nm_axpy2(n, 0.25, x.data_ptr(), -0.5, z.data_ptr(), w.data_ptr(),
+                                      s),
+        "dot": lambda: lib.nm_dot(n, x.data_ptr(), w.data_ptr(), C.byref(res), s),
+    }
+    # inputs (3 x 33 MB) are smaller than L2: a 256 MB write before each round
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    ops = {"flush": flush.zero_, **ops}
+    with ClockSampler(local_rank) as clk:
+        total_ms, avg = time_ops(ops, stream, args.steps, args.warmup)
+    step_ms = avg["axpy"] + avg["axpy2"] + avg["dot"]
+    step_ms = max_over_ranks([step_ms], world, dev)[0]
+    if rank != 0:
+        return None
+    nbytes = vec_bytes(n)
+    peak, peak_src = measured_peak()
+    config = {"workload": desc, "name": args.workload, "n": n, "bytes_per_step": nbytes,
+              "bytes_formula": "axpy 24n + axpy2 24n + dot 16n",
+              "l2": "operands (3 x 33 MB) smaller than L2: L2 flushed (256 MB write) before "
+                    "each round, ops timed alone",
+              "parallelism": f"replicas x{world}",
+              "api": "C ABI nm_axpy / nm_axpy2 / nm_dot (the dot returns its value to the "
+                     "host, as vec_local_dot does)"}
+    line = base_line(args, world, round(world * nbytes / (step_ms * 1e-3) / 1e9, 2), "GB/s",
+                     step_ms, precision, config)
+    per = {k: {"us": round(avg[k] * 1e3, 2),
+               "gbs": round((24 if k != "dot" else 16) * n / (avg[k] * 1e-3) / 1e9, 1)}
+           for k in ("axpy", "axpy2", "dot")}
+    line.update({
+        "roofline": {"bound": "hbm", "achieved": per["axpy2"]["gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": round(per["axpy2"]["gbs"] / peak, 4),
+                     "peak_source": peak_src, "traffic": None,
+                     "kernel": "nm::axpy2_kernel (24 B per element)", "per_op": per},
+        "e2e": {"value": line["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8,
+                "note": "the dot's value comes back to the host every step; the vectors are "
+                        "device operands of the CG, never host data"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    })
+    return line
+
+
+def run_halo(args, rank, world, local_rank):
+    import torch
+
+    from num_b200 import _lib
+    dev = torch.device("cuda", local_rank)
+    desc, _, precision = WORKLOADS[args.workload]
+    A, parts = halo_workload()
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    rp, ci, v = (np.ascontiguousarray(a) for a in (A.row_ptr, A.col_idx, A.values))
+    x = torch.tensor(np.random.default_rng(6).uniform(-1, 1, A.ncols), device=dev)
+    handles, bufs = [], []
+    for r, p in enumerate(parts):
+        h = C.c_void_p()
+        _lib.check(lib.nm_dist_create(rp.ctypes.data, ci.ctypes.data, v.ctypes.data, A.nrows,
+                                      A.ncols, r, len(parts), C.byref(h)), "nm_dist_create")
+        handles.append(h)
+        send = torch.empty(max(p["total_send"], 1), dtype=torch.float64, device=dev)
+        recv = torch.rand(max(p["n_ghost"], 1), dtype=torch.float64, device=dev)
+        ext = torch.empty(p["local_n"] + p["n_ghost"], dtype=torch.float64, device=dev)
+        bufs.append((x[p["row_start"]:p["row_end"]], send, recv, ext))
+    ops = {}
+    for r, (h, (xl, send, recv, ext)) in enumerate(zip(handles, bufs)):
+        ops[f"pack{r}"] = (lambda h=h, xl=xl, send=send:
+                           lib.nm_halo_pack(h, xl.data_ptr(), send.data_ptr(), s))
+        ops[f"unpack{r}"] = (lambda h=h, recv=recv, ext=ext:
+                             lib.nm_halo_unpack(h, recv.data_ptr(), ext.data_ptr(), s))
+    with ClockSampler(local_rank) as clk:
+        total_ms, avg = time_ops(ops, stream, args.steps, args.warmup)
+    step_ms = sum(avg.values())
+    step_ms = max_over_ranks([step_ms], world, dev)[0]
+    for h in handles:
+        lib.nm_dist_destroy(h)
+    if rank != 0:
+        return None
+    nbytes = sum(halo_bytes(p["total_send"], p["n_ghost"]) for p in parts)
+    pack_us = sum(avg[f"pack{r}"] for r in range(len(parts))) * 1e3
+    unpack_us = sum(avg[f"unpack{r}"] for r in range(len(parts))) * 1e3
+    pack_b = sum(p["total_send"] * 20 for p in parts)
+    peak, peak_src = measured_peak()
+    pack_gbs = pack_b / (pack_us * 1e-6) / 1e9
+    config = {"workload": desc, "name": args.workload, "ranks": len(parts),
+              "send_total": sum(p["total_send"] for p in parts),
+              "ghost_total": sum(p["n_ghost"] for p in parts), "bytes_per_step": nbytes,
+              "bytes_formula": "pack 20 B per sent value + unpack 16 B per ghost",
+              "parallelism": f"replicas x{world}",
+              "api": "C ABI nm_halo_pack / nm_halo_unpack on nm_dist_create slabs"}
+    line = base_line(args, world, round(world * nbytes / (step_ms * 1e-3) / 1e9, 2), "GB/s",
+                     step_ms, precision, config)
+    line.update({
+        "roofline": {"bound": "hbm", "achieved": round(pack_gbs, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(pack_gbs / peak, 4), "peak_source": peak_src,
+                     "traffic": None, "kernel": "nm::halo_pack_kernel",
+                     "pack_us_per_step": round(pack_us, 2),
+                     "unpack_us_per_step": round(unpack_us, 2),
+                     "note": "each launch moves ~0.5-1 MB: launch latency, not bandwidth, "
+                             "bounds it"},
+        "e2e": {"value": line["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0,
+                "note": "halo buffers are device operands of the distributed SpMV"},
+        "gpu_launches": 2 * len(parts) * args.steps,
+        "clocks": clk.summary(),
+    })
+    return line
+
+
+DEFAULT_STEPS = {"spmv": 2000, "batch": 100, "cg": 50, "engine": 5, "serve": 3, "vec": 200,
+                 "halo": 200}
 
 
 def main():
@@ -1375,7 +1620,7 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     try:
         run = {"spmv": run_spmv, "batch": run_batch, "cg": run_cg, "engine": run_engine,
-               "serve": run_serve}[kind]
+               "serve": run_serve, "vec": run_vec, "halo": run_halo}[kind]
         line = run(args, rank, world, local_rank)
     finally:
         if world > 1:
