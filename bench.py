@@ -738,7 +738,10 @@ CG_PATHS = {0: "CUDA-graph chunks of 3 kernels per iteration",
             1: "persistent TMA-pipelined solve, 3 grid barriers per iteration",
             2: "persistent TMA-pipelined solve, 2 grid barriers per iteration",
             3: "resident solve (matrix rows and vectors on chip, 2 grid-wide sums per "
-               "iteration)"}
+               "iteration)",
+            4: "cluster solve (one 16-CTA thread-block cluster: matrix values in shared "
+               "memory, the direction read over distributed shared memory, 3 hardware "
+               "cluster barriers per iteration)"}
 
 
 def run_cg(args, rank, world, local_rank):
@@ -1580,7 +1583,7 @@ def main():
                     help="serve_c5: the engine's preconditioner")
     ap.add_argument("--no-plain", action="store_true",
                     help="serve_c5: skip the plain FP64 drop-in comparison")
-    ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2, 3],
+    ap.add_argument("--cg-mode", type=int, default=1, choices=[0, 1, 2, 3, 4],
                     help="nm_cg_set_persistent: 1 persistent (default), 2 the TMA-pipelined "
                          "persistent solve only, 3 the resident solve only, 0 CUDA-graph "
                          "chunks")

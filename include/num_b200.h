@@ -230,7 +230,11 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
  * is co-resident, else the resident solve (matrix rows and vectors kept on
  * chip, two grid-wide sums per iteration; rows of at most 8 nonzeros);
  * 2 the TMA-pipelined persistent solve only; 3 the resident solve only;
- * 0 CUDA-graph chunks of three kernels per iteration.  All give the same
+ * 4 the cluster solve only (systems of at most 65,536 rows of at most 8
+ * nonzeros on one 16-CTA thread-block cluster: matrix values in shared
+ * memory, the direction read over distributed shared memory, hardware
+ * cluster barriers); 0 CUDA-graph chunks of three kernels per iteration
+ * (also what 2 to 4 run where their path does not apply).  All give the same
  * iterates, bit for bit (every dot product is summed in one fixed order: per
  * row block or 256-row tile, then over the blocks).  Other values:
  * NM_ERR_INVALID.  No reference counterpart (an implementation switch). */
@@ -239,7 +243,8 @@ int nm_cg_set_persistent(int32_t enable);
 /* How the last nm_cg_local / nm_dist_cg_single solve on A iterated: 0 the
  * CUDA-graph chunks, 1 the TMA-pipelined persistent solve (three grid
  * barriers per iteration), 2 the same in its two-barrier form, 3 the resident
- * solve; -1 before A's first solve.  No reference counterpart. */
+ * solve, 4 the cluster solve; -1 before A's first solve.  No reference
+ * counterpart. */
 int nm_cg_last_path(const nm_csr* A, int32_t* path);
 
 /* cg_solve_local (src/cg_solver.hpp:133-196; src/bindings.cpp:273-290):

@@ -527,6 +527,8 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
             st = plan_resident(A, ws.get());
             if (st != NM_OK) return st;
         }
+        st = plan_cluster(A, ws.get());
+        if (st != NM_OK) return st;
     }
     ws->err = device_error_word();
     if (!ws->err) return fail(NM_ERR_CUDA, "cg: cannot map the device error word");
@@ -656,13 +658,16 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
     // mode 1: the TMA-pipelined persistent solve where it fits (9.8 us per
     // iteration on the 256^2 Laplacian against 10.8 us resident), else the
     // resident one; 2: the former only; 3: the latter only; 0: graph chunks
-    const bool resident = ws->resident && (mode == 3 || (mode == 1 && !ws->coop));
-    const bool coop = resident || (ws->coop && (mode == 1 || mode == 2));
+    // 4: the cluster solve only
+    const bool cluster = ws->cluster && mode == 4;
+    const bool resident = !cluster && ws->resident && (mode == 3 || (mode == 1 && !ws->coop));
+    const bool coop = cluster || resident || (ws->coop && (mode == 1 || mode == 2));
     if (coop) {
         // the whole iteration loop in one persistent launch
-        st = resident ? launch_resident(A, ws, s) : launch_coop(A, ws, s);
+        st = cluster ? launch_cluster(A, ws, s)
+                     : (resident ? launch_resident(A, ws, s) : launch_coop(A, ws, s));
         if (st != NM_OK) return st;
-        ws->last_path = resident ? 3 : (ws->coop_formed ? 2 : 1);
+        ws->last_path = cluster ? 4 : (resident ? 3 : (ws->coop_formed ? 2 : 1));
         NM_CUDA_TRY(cudaMemcpyAsync(ws->h_out, ws->st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         NM_CUDA_TRY(cudaStreamSynchronize(s));
     }
@@ -703,8 +708,8 @@ extern "C" int nm_cg_last_path(const nm_csr* A, int32_t* path) {
 
 extern "C" int nm_cg_set_persistent(int32_t enable) {
     nm::clear_error();
-    if (enable < 0 || enable > 3)
-        return nm::fail(NM_ERR_INVALID, "nm_cg_set_persistent: 0, 1, 2 or 3");
+    if (enable < 0 || enable > 4)
+        return nm::fail(NM_ERR_INVALID, "nm_cg_set_persistent: 0 to 4");
     nm::g_cg_persistent.store(enable);
     return NM_OK;
 }

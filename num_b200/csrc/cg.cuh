@@ -56,8 +56,19 @@ struct CgWorkspace {
     void* res_mem = nullptr;      // per-CTA row / window ranges and the sum slots
     int4* res_cta = nullptr;
     double* res_slots = nullptr;
+    // the cluster solve (cg_cluster.cu), when the matrix qualifies
+    bool cluster = false;
+    int cl_rows_per_thread = 0, cl_width = 0;
+    size_t cl_smem = 0;
     ~CgWorkspace();
 };
+
+// The cluster solve: systems of at most 65,536 rows of at most 8 nonzeros
+// whose row blocks are whole 256-row tiles, on one cluster of 16 CTAs when
+// the device can schedule it.  NM_OK with ws->cluster false when it cannot.
+int plan_cluster(const nm_csr* A, CgWorkspace* ws);
+// One cluster solve on `s` after cg_init_kernel (ws->r, ws->p hold r0 = p0).
+int launch_cluster(const nm_csr* A, CgWorkspace* ws, cudaStream_t s);
 
 // The resident solve: systems of at most kResidentMaxRows rows whose row
 // blocks are whole 256-row tiles, at most kResidentMaxTiles tiles per CTA,

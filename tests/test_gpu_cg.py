@@ -298,7 +298,7 @@ def test_persistent_and_graph_paths_bit_identical(kspmv, nmlib, case):
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
     out = []
     try:
-        for persistent in (1, 0, 2, 3, 1):
+        for persistent in (1, 0, 2, 3, 4, 1):
             nmlib.nm_cg_set_persistent(persistent)
             x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
             info = kspmv.cg_solve_local(M, b, x, tol=1e-9, max_iter=3000)
@@ -326,3 +326,28 @@ def test_large_system_graph_path(kspmv, oracle, offset):
     assert info["converged"] and abs(info["iters"] - oinfo["iters"]) <= 1
     xs = x.cpu().numpy()
     assert np.linalg.norm(xs - ox) <= 1e-9 * np.linalg.norm(ox)
+
+
+def test_cluster_solve_c1(kspmv, nmlib, oracle):
+    # The 256^2 Laplacian on one 16-CTA cluster (where the device schedules
+    # it): the oracle's 454 iterations, the graph path's bits.
+    import ctypes as C
+    A = gen.laplacian_2d(256)
+    b = torch.tensor(oracle.spmv(A.row_ptr, A.col_idx, A.values, np.ones(A.ncols)),
+                     device="cuda")
+    M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
+    out = []
+    try:
+        for mode in (4, 0, 4):
+            nmlib.nm_cg_set_persistent(mode)
+            x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
+            info = kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=5000)
+            path = C.c_int32(-1)
+            nmlib.nm_cg_last_path(M._h, C.byref(path))
+            out.append((info, x.cpu().numpy(), path.value))
+    finally:
+        nmlib.nm_cg_set_persistent(1)
+    assert out[0][2] in (0, 4) and out[1][2] == 0
+    for info, x, _ in out:
+        assert info["iters"] == 454 and info["converged"]
+        assert np.array_equal(x, out[1][1])
