@@ -422,6 +422,7 @@ CgWorkspace::~CgWorkspace() {
     if (cap_stream) cudaStreamDestroy(cap_stream);
     cudaFree(dmem);
     if (res_mem) cudaFree(res_mem);
+    if (cl_mem) cudaFree(cl_mem);
     pinned_slots().put(h_in);
     pinned_slots().put(h_out);
 }

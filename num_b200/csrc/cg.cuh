@@ -58,14 +58,21 @@ struct CgWorkspace {
     double* res_slots = nullptr;
     // the cluster solve (cg_cluster.cu), when the matrix qualifies
     bool cluster = false;
-    int cl_rows_per_thread = 0, cl_width = 0;
+    int cl_rows_per_thread = 0, cl_width = 0, cl_class = 0, cl_halo = 0, cl_pmax = 0;
+    bool cl_f32v = false;  // A's values held as floats (each a float exactly)
     size_t cl_smem = 0;
+    void* cl_mem = nullptr;  // renumbered columns and the halo store lists
+    uint16_t* cl_lcol = nullptr;
+    int32_t* cl_push_off = nullptr;
+    uint32_t* cl_push_ent = nullptr;
     ~CgWorkspace();
 };
 
-// The cluster solve: systems of at most 65,536 rows of at most 8 nonzeros
-// whose row blocks are whole 256-row tiles, on one cluster of 16 CTAs when
-// the device can schedule it.  NM_OK with ws->cluster false when it cannot.
+// The cluster solve: systems whose row blocks are whole 256-row tiles, of at
+// most 65,536 rows of at most 5 nonzeros (49,152 of 7 or 8 when every value
+// is a float exactly, 40,960 otherwise), on one cluster of 16 CTAs when the
+// device can schedule it and the rows fit its shared memory.  NM_OK with
+// ws->cluster false when it cannot.
 int plan_cluster(const nm_csr* A, CgWorkspace* ws);
 // One cluster solve on `s` after cg_init_kernel (ws->r, ws->p hold r0 = p0).
 int launch_cluster(const nm_csr* A, CgWorkspace* ws, cudaStream_t s);

@@ -328,11 +328,28 @@ def test_large_system_graph_path(kspmv, oracle, offset):
     assert np.linalg.norm(xs - ox) <= 1e-9 * np.linalg.norm(ox)
 
 
-def test_cluster_solve_c1(kspmv, nmlib, oracle):
-    # The 256^2 Laplacian on one 16-CTA cluster (where the device schedules
-    # it): the oracle's 454 iterations, the graph path's bits.
+def _tridiag(n):
+    # 1-D Laplacian: 2 on the diagonal, -1 beside it (3 nonzeros per row)
+    rows = np.repeat(np.arange(n), 3)
+    cols = (rows + np.tile([-1, 0, 1], n))
+    keep = (cols >= 0) & (cols < n)
+    rows, cols = rows[keep], cols[keep]
+    vals = np.where(rows == cols, 2.0, -1.0)
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, rows + 1, 1)
+    return gen.Csr(np.cumsum(rp, dtype=np.int32), cols.astype(np.int32), vals, n, n)
+
+
+@pytest.mark.parametrize("case", ["c1_256sq", "lap3d_32", "lap2d_40", "tridiag_3000"])
+def test_cluster_solve(kspmv, nmlib, oracle, case):
+    # Systems the 16-CTA cluster solve takes (where the device schedules it):
+    # the 256^2 Laplacian (5 nonzeros, 8 rows per thread: the full cluster),
+    # 32^3 (7 nonzeros, 4 rows per thread), 40^2 (a partial last tile, 1 row
+    # per thread) and a 1-D Laplacian (3 nonzeros).  The graph path's bits and
+    # the oracle's iteration count (454 on the 256^2 system, exactly).
     import ctypes as C
-    A = gen.laplacian_2d(256)
+    A = {"c1_256sq": lambda: gen.laplacian_2d(256), "lap3d_32": lambda: gen.laplacian_3d(32),
+         "lap2d_40": lambda: gen.laplacian_2d(40), "tridiag_3000": lambda: _tridiag(3000)}[case]()
     b = torch.tensor(oracle.spmv(A.row_ptr, A.col_idx, A.values, np.ones(A.ncols)),
                      device="cuda")
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
@@ -341,13 +358,19 @@ def test_cluster_solve_c1(kspmv, nmlib, oracle):
         for mode in (4, 0, 4):
             nmlib.nm_cg_set_persistent(mode)
             x = torch.zeros(A.nrows, dtype=torch.float64, device="cuda")
-            info = kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=5000)
+            info = kspmv.cg_solve_local(M, b, x, tol=1e-8, max_iter=20000)
             path = C.c_int32(-1)
             nmlib.nm_cg_last_path(M._h, C.byref(path))
             out.append((info, x.cpu().numpy(), path.value))
     finally:
         nmlib.nm_cg_set_persistent(1)
-    assert out[0][2] in (0, 4) and out[1][2] == 0
+    assert out[0][2] in (0, 4) and out[1][2] == 0 and out[2][2] == out[0][2]
+    oinfo, _ = oracle.cg_local(A.row_ptr, A.col_idx, A.values, b.cpu().numpy(), tol=1e-8,
+                               max_iter=20000)
     for info, x, _ in out:
-        assert info["iters"] == 454 and info["converged"]
+        assert info["converged"] and info["iters"] == out[1][0]["iters"]
+        assert info["residual"] == out[1][0]["residual"]
         assert np.array_equal(x, out[1][1])
+    assert abs(out[1][0]["iters"] - oinfo["iters"]) <= 1
+    if case == "c1_256sq":
+        assert out[1][0]["iters"] == 454
