@@ -225,19 +225,21 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
 /* ---- CG -------------------------------------------------------------------- */
 
 /* Process-wide choice of how nm_cg_local / nm_dist_cg_single iterate:
- * 1 (default) one persistent cooperative launch per solve for systems of at
- * most 262,144 rows -- the TMA-pipelined persistent solve where its SpMV grid
- * is co-resident, else the resident solve (matrix rows and vectors kept on
+ * 1 (default) one persistent launch per solve for systems of at most 262,144
+ * rows -- the cluster solve where it applies (systems of at most 65,536 rows
+ * of at most 8 nonzeros on one 16-CTA thread-block cluster: the rows of A in
+ * shared memory, each CTA's halo of the direction kept current over
+ * distributed shared memory, two hardware cluster barriers per iteration),
+ * else the TMA-pipelined persistent solve where its SpMV grid is
+ * co-resident, else the resident solve (matrix rows and vectors kept on
  * chip, two grid-wide sums per iteration; rows of at most 8 nonzeros);
  * 2 the TMA-pipelined persistent solve only; 3 the resident solve only;
- * 4 the cluster solve only (systems of at most 65,536 rows of at most 8
- * nonzeros on one 16-CTA thread-block cluster: matrix values in shared
- * memory, the direction read over distributed shared memory, hardware
- * cluster barriers); 0 CUDA-graph chunks of three kernels per iteration
- * (also what 2 to 4 run where their path does not apply).  All give the same
- * iterates, bit for bit (every dot product is summed in one fixed order: per
- * row block or 256-row tile, then over the blocks).  Other values:
- * NM_ERR_INVALID.  No reference counterpart (an implementation switch). */
+ * 4 the cluster solve only; 0 CUDA-graph chunks of three kernels per
+ * iteration (also what 2 to 4 run where their path does not apply).  All
+ * give the same iterates, bit for bit (every dot product is summed in one
+ * fixed order: per row block or 256-row tile, then over the blocks).  Other
+ * values: NM_ERR_INVALID.  No reference counterpart (an implementation
+ * switch). */
 int nm_cg_set_persistent(int32_t enable);
 
 /* How the last nm_cg_local / nm_dist_cg_single solve on A iterated: 0 the

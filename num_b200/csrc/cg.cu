@@ -656,11 +656,11 @@ int cg_run(nm_csr* A, const double* b, double* x, double tol, int32_t max_iter, 
     NM_CHECK_LAUNCH();
 
     const int mode = g_cg_persistent.load();
-    // mode 1: the TMA-pipelined persistent solve where it fits (9.8 us per
-    // iteration on the 256^2 Laplacian against 10.8 us resident), else the
-    // resident one; 2: the former only; 3: the latter only; 0: graph chunks
-    // 4: the cluster solve only
-    const bool cluster = ws->cluster && mode == 4;
+    // mode 1: the cluster solve where it applies (6.0 us per iteration on the
+    // 256^2 Laplacian), else the TMA-pipelined persistent solve where it fits
+    // (9.8 us there), else the resident one (10.8 us); 2, 3, 4: the second,
+    // the third, the first only; 0: graph chunks
+    const bool cluster = ws->cluster && (mode == 4 || mode == 1);
     const bool resident = !cluster && ws->resident && (mode == 3 || (mode == 1 && !ws->coop));
     const bool coop = cluster || resident || (ws->coop && (mode == 1 || mode == 2));
     if (coop) {

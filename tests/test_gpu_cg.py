@@ -264,10 +264,11 @@ def _arrow_spd(n, rng):
     return gen.Csr(rp, ci, v, n, n)
 
 
-# Mode 1 runs the resident solve where it applies (the 256^2 and 40^3
-# Laplacians and the 48^3 variable-coefficient system: rows of <= 8 nonzeros,
-# whole 256-row tiles) and the TMA-pipelined persistent solve elsewhere; mode 2
-# forces the latter, which runs in its two-barrier form (direction formed
+# Mode 1 runs the cluster solve where it applies (the 256^2 Laplacian), else
+# the TMA-pipelined persistent solve where its grid is co-resident, else the
+# resident solve where that applies (rows of <= 8 nonzeros, whole 256-row
+# tiles); modes 3 and 4 force the resident and the cluster solve where they
+# apply; mode 2 forces the TMA-pipelined one, which runs in its two-barrier form (direction formed
 # inside the SpMV) while the SpMV grid fits it -- the 256^2 and 40^3
 # Laplacians, the 30,000-row banded system (scattered off-band columns: the
 # gather path) and the arrow matrix (a long row) -- and in its three-barrier
