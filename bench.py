@@ -1457,7 +1457,12 @@ def run_vec(args, rank, world, local_rank):
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
     ops = {"flush": flush.zero_, **ops}
     with ClockSampler(local_rank) as clk:
-        sustained(lambda: [f() for f in ops.values()], stream, dev)
+        # ~0.5 s of back-to-back rounds (the dot synchronises each one) so the
+        # sampler sees the GPU under this load for 20+ samples
+        t_end = time.perf_counter() + 0.5
+        while time.perf_counter() < t_end:
+            for f in ops.values():
+                f()
         total_ms, avg = time_ops(ops, stream, args.steps, args.warmup)
     step_ms = avg["axpy"] + avg["axpy2"] + avg["dot"]
     step_ms = max_over_ranks([step_ms], world, dev)[0]

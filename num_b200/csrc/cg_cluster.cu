@@ -151,8 +151,8 @@ __device__ __forceinline__ void push_tiles(double (*scr)[kWarps], uint32_t ts_sa
 }
 
 // After the cluster barrier: the total of the cluster's tile sums (this
-// CTA's copy `ts`, nblk <= 256 of them) in reduce256's order, by every warp
-// on its own -- lane l takes tiles l + 32 w as virtual warp w's lane, the
+// CTA's copy `ts`, nblk <= 256 of them) in reduce256's order, by one warp --
+// lane l takes tiles l + 32 w as virtual warp w's lane, the
 // eight virtual warps' trees run at once and their sums are added in order
 // from 0.0, block_sum8's order.
 __device__ __forceinline__ double cluster_total(const double* ts, int nblk) {
