@@ -272,8 +272,10 @@ int nm_cg_local(nm_csr* A, const double* b, double* x, double tol, int32_t max_i
  * A is a handle made earlier with nm_csr_create; b, x as in nm_cg_local.
  * Limit: A->nrows <= 262,144 (larger matrices: NM_ERR_INVALID).  The first
  * call on a device looks up the array's device address, and the first call
- * with each tile / stage setting sets that kernel's attributes; make those
- * first calls before any stream capture.  All calls
+ * with each tile / stage setting sets that kernel's attributes; those first
+ * calls must not overlap a global-mode stream capture on any thread.  The
+ * entry point waits on `stream` for the solve's progress, so it cannot be
+ * called on a stream that is being captured.  All calls
  * share the one array (the state is reset at the start of each call); calls
  * that overlap on the GPU would race, so this entry point serialises its host
  * callers and synchronises `stream` before returning, on error returns too. */

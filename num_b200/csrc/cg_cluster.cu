@@ -34,7 +34,9 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
-#include <unordered_map>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -455,11 +457,12 @@ int plan_cluster(const nm_csr* A, CgWorkspace* ws) {
     // halo slot per other column it reads; and for every such slot a store
     // by the thread that owns the column's row.
     std::vector<uint16_t> lcol(static_cast<size_t>(nnz));
-    std::vector<std::vector<uint32_t>> by_thread(size_t(kClusterCtas) * NT);
+    std::vector<int32_t> slot_of(static_cast<size_t>(n), -1);  // a CTA's halo slot of a column
+    std::vector<int32_t> touched;
+    std::vector<std::pair<int32_t, uint32_t>> pushes;  // (owner CTA * NT + thread, entry)
     int32_t halo = 0;
     for (int c = 0; c < kClusterCtas; ++c) {
         const int64_t r0 = int64_t(c) * RC, r1 = std::min<int64_t>(r0 + RC, n);
-        std::unordered_map<int32_t, int32_t> slot_of;
         for (int64_t i = r0; i < r1; ++i)
             for (int32_t z = rp[i]; z < rp[i + 1]; ++z) {
                 const int32_t col = ci[z];
@@ -467,30 +470,38 @@ int plan_cluster(const nm_csr* A, CgWorkspace* ws) {
                     lcol[size_t(z)] = static_cast<uint16_t>(col - r0);
                     continue;
                 }
-                const auto ins = slot_of.emplace(col, int32_t(slot_of.size()));
-                const int32_t slot = ins.first->second;
-                if (RC + slot > 0xffff) return NM_OK;  // beyond 16-bit column numbers
-                lcol[size_t(z)] = static_cast<uint16_t>(RC + slot);
-                if (ins.second) {
+                int32_t slot = slot_of[size_t(col)];
+                if (slot < 0) {
+                    slot = int32_t(touched.size());
+                    if (RC + slot > 0xffff) return NM_OK;  // beyond 16-bit column numbers
+                    slot_of[size_t(col)] = slot;
+                    touched.push_back(col);
                     const int32_t o = col / RC, lr = col - o * RC;
-                    by_thread[size_t(o) * NT + size_t(lr % NT)].push_back(
-                        uint32_t(lr / NT) | uint32_t(c) << 3 | uint32_t(slot) << 7);
+                    pushes.emplace_back(o * NT + lr % NT,
+                                        uint32_t(lr / NT) | uint32_t(c) << 3 | uint32_t(slot) << 7);
                 }
+                lcol[size_t(z)] = static_cast<uint16_t>(RC + slot);
             }
-        halo = std::max(halo, int32_t(slot_of.size()));
+        halo = std::max(halo, int32_t(touched.size()));
+        for (const int32_t col : touched) slot_of[size_t(col)] = -1;
+        touched.clear();
     }
-    std::vector<int32_t> push_off(size_t(kClusterCtas) * (NT + 1));
-    std::vector<uint32_t> push_ent;
+    // the stores grouped by owning thread (counting sort; each thread's in
+    // the order found)
+    std::vector<int32_t> push_off(size_t(kClusterCtas) * (NT + 1), 0);
+    std::vector<int32_t> per_thread(size_t(kClusterCtas) * NT + 1, 0);
+    for (const auto& pr : pushes) ++per_thread[size_t(pr.first) + 1];
+    for (size_t k = 1; k < per_thread.size(); ++k) per_thread[k] += per_thread[k - 1];
+    std::vector<uint32_t> push_ent(pushes.size());
+    {
+        std::vector<int32_t> fill(per_thread.begin(), per_thread.end() - 1);
+        for (const auto& pr : pushes) push_ent[size_t(fill[size_t(pr.first)]++)] = pr.second;
+    }
     int32_t pmax = 0;
     for (int o = 0; o < kClusterCtas; ++o) {
-        const size_t first = push_ent.size();
-        for (int t = 0; t < NT; ++t) {
-            push_off[size_t(o) * (NT + 1) + t] = int32_t(push_ent.size());
-            const auto& v = by_thread[size_t(o) * NT + t];
-            push_ent.insert(push_ent.end(), v.begin(), v.end());
-        }
-        push_off[size_t(o) * (NT + 1) + NT] = int32_t(push_ent.size());
-        pmax = std::max(pmax, int32_t(push_ent.size() - first));
+        for (int t = 0; t <= NT; ++t)
+            push_off[size_t(o) * (NT + 1) + t] = per_thread[size_t(o) * NT + t];
+        pmax = std::max(pmax, per_thread[size_t(o + 1) * NT] - per_thread[size_t(o) * NT]);
     }
     if (pmax > kMaxPushes) return NM_OK;
 
@@ -504,27 +515,46 @@ int plan_cluster(const nm_csr* A, CgWorkspace* ws) {
     NM_CUDA_TRY(cudaDeviceGetAttribute(&cl, cudaDevAttrClusterLaunch, dev));
     NM_CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const void* fn = cluster_kernel_for(f32v, cls, R);
-    cudaFuncAttributes fa;
-    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
-    if (!cl || smem + fa.sharedSizeBytes > size_t(smem_max)) return NM_OK;
-    NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kClusterCtas);
-    cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = kClusterCtas;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) != cudaSuccess || clusters < 1) {
-        cudaGetLastError();  // not schedulable here: the other paths run
-        return NM_OK;
+    if (!cl) return NM_OK;
+    // Per device and kernel instance, once: its static shared memory, the
+    // cluster-size and shared-memory attributes (set to the device's
+    // maximum), and per dynamic size whether a cluster can be scheduled.
+    static std::mutex cache_mu;
+    static std::map<std::pair<int, const void*>, size_t> static_smem;
+    static std::map<std::tuple<int, const void*, size_t>, bool> schedulable;
+    std::lock_guard<std::mutex> lock(cache_mu);
+    auto si = static_smem.find({dev, fn});
+    if (si == static_smem.end()) {
+        cudaFuncAttributes fa;
+        NM_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+        NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        NM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem_max - static_cast<int>(fa.sharedSizeBytes)));
+        si = static_smem.emplace(std::make_pair(dev, fn), fa.sharedSizeBytes).first;
+    }
+    if (smem + si->second > size_t(smem_max)) return NM_OK;
+    const auto key = std::make_tuple(dev, fn, smem);
+    auto sc = schedulable.find(key);
+    if (sc != schedulable.end()) {
+        if (!sc->second) return NM_OK;
+    } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kClusterCtas);
+        cfg.blockDim = dim3(NT);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = kClusterCtas;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        const bool ok = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) == cudaSuccess &&
+                        clusters >= 1;
+        if (!ok) cudaGetLastError();  // not schedulable here: the other paths run
+        schedulable.emplace(key, ok);
+        if (!ok) return NM_OK;
     }
 
     // column numbers, push offsets and entries in one device allocation

@@ -341,16 +341,34 @@ def _tridiag(n):
     return gen.Csr(np.cumsum(rp, dtype=np.int32), cols.astype(np.int32), vals, n, n)
 
 
-@pytest.mark.parametrize("case", ["c1_256sq", "lap3d_32", "lap2d_40", "tridiag_3000"])
+def _shifted_laplacian_2d(L, shift):
+    # 2-D Laplacian with shift(i) added to the diagonal of row i
+    A = gen.laplacian_2d(L)
+    v = A.values.copy()
+    for i in range(A.nrows):
+        for z in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            if A.col_idx[z] == i:
+                v[z] += shift(i)
+    return gen.Csr(A.row_ptr, A.col_idx, v, A.nrows, A.ncols)
+
+
+@pytest.mark.parametrize("case", ["c1_256sq", "lap3d_32", "lap2d_40", "tridiag_3000",
+                                  "intdiag_100", "randdiag_120"])
 def test_cluster_solve(kspmv, nmlib, oracle, case):
     # Systems the 16-CTA cluster solve takes (where the device schedules it):
-    # the 256^2 Laplacian (5 nonzeros, 8 rows per thread: the full cluster),
-    # 32^3 (7 nonzeros, 4 rows per thread), 40^2 (a partial last tile, 1 row
-    # per thread) and a 1-D Laplacian (3 nonzeros).  The graph path's bits and
-    # the oracle's iteration count (454 on the 256^2 system, exactly).
+    # the 256^2 Laplacian (5 nonzeros, 1,024 threads x 4 rows: the full
+    # cluster), 32^3 (7 nonzeros), 40^2 (a partial last tile) and a 1-D
+    # Laplacian (3 nonzeros), whose few distinct values the CTAs hold as
+    # dictionary indices; a 100^2 Laplacian with integer diagonals 4..10
+    # (floats exactly, more than 4 distinct: held as floats) and a 120^2 one
+    # with random diagonals (held as doubles, 512 threads).  The graph path's
+    # bits and the oracle's iteration count (454 on the 256^2 system, exactly).
     import ctypes as C
+    rng = np.random.default_rng(41)
     A = {"c1_256sq": lambda: gen.laplacian_2d(256), "lap3d_32": lambda: gen.laplacian_3d(32),
-         "lap2d_40": lambda: gen.laplacian_2d(40), "tridiag_3000": lambda: _tridiag(3000)}[case]()
+         "lap2d_40": lambda: gen.laplacian_2d(40), "tridiag_3000": lambda: _tridiag(3000),
+         "intdiag_100": lambda: _shifted_laplacian_2d(100, lambda i: float(i % 7)),
+         "randdiag_120": lambda: _shifted_laplacian_2d(120, lambda i: rng.uniform(0, 1))}[case]()
     b = torch.tensor(oracle.spmv(A.row_ptr, A.col_idx, A.values, np.ones(A.ncols)),
                      device="cuda")
     M = kspmv.upload_csr(A.row_ptr, A.col_idx, A.values, A.nrows, A.ncols)
