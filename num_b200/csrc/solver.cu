@@ -307,6 +307,75 @@ __device__ __forceinline__ double2 ordered_sum256(const double* part, int64_t lo
     return out;
 }
 
+// ordered_sum256 computed by a CTA of 1024 threads, the same bits: thread
+// t + 256 g (g < 4) forms accumulators 2g and 2g + 1 of ordered_sum256's
+// thread t -- the entries lo + t + 256 (8 m + k) in increasing m, as there --
+// so the loads go out in one round instead of one round per 8 entries; the
+// accumulators then meet in shared memory (acc: 8 x 256 entries) and thread
+// t < 256 combines its eight in ordered_sum256's tree, then its warp and
+// warp order.  Every thread calls it and gets the result.
+template <bool PAIRS>
+__device__ __forceinline__ double2 ordered_sum256_wide(const double* part, int64_t lo,
+                                                       int64_t hi, double2 (*acc)[kThreads],
+                                                       double2* scratch) {
+    const int t = threadIdx.x & (kThreads - 1), g = threadIdx.x / kThreads;
+    auto ld = [&](int64_t i) -> double2 {
+        if (PAIRS) return __ldcg(reinterpret_cast<const double2*>(part) + i);
+        return make_double2(__ldcg(part + i), 0.0);
+    };
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int k = 2 * g + h;
+        double ax = 0.0, ay = 0.0;
+        // accumulator k's entries in increasing m, eight loads at a time
+        constexpr int64_t kStride = 8 * int64_t(kThreads);
+        for (int64_t e = lo + t + int64_t(kThreads) * k; e < hi; e += 8 * kStride) {
+            double2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int64_t j = e + q * kStride;
+                v[q] = j < hi ? ld(j) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (e + q * kStride < hi) {
+                    ax += v[q].x;
+                    ay += v[q].y;
+                }
+        }
+        acc[k][t] = make_double2(ax, ay);
+    }
+    __syncthreads();
+    double sx = 0.0, sy = 0.0;
+    if (threadIdx.x < kThreads) {
+        double a[8], b[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a[k] = acc[k][t].x;
+            b[k] = acc[k][t].y;
+        }
+        sx = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+        sy = ((b[0] + b[1]) + (b[2] + b[3])) + ((b[4] + b[5]) + (b[6] + b[7]));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    if (lane == 0 && warp < kWarps) scratch[warp] = make_double2(sx, sy);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 tt = make_double2(0.0, 0.0);
+        for (int w = 0; w < kWarps; ++w) {
+            tt.x += scratch[w].x;
+            tt.y += scratch[w].y;
+        }
+        scratch[kWarps] = tt;
+    }
+    __syncthreads();
+    const double2 out = scratch[kWarps];
+    __syncthreads();  // scratch and acc are free for the next call
+    return out;
+}
+
 // ---- per-system scalar steps (one CTA per system of the outer list) ----------------
 
 enum ScalarKind { kOuterNorm = 2, kStart = 3 };
@@ -376,31 +445,35 @@ __global__ void __launch_bounds__(kScalarThreads)
 // (after the SpMV), and the stopping test and beta from the tile sums (after
 // the update), one CTA per system; the same formulas as the tile kernels use
 // for small systems.
-// (256-thread CTAs: the sums are those every path forms, ordered_sum256.)
-__global__ void __launch_bounds__(kThreads)
+// (1024-thread CTAs forming the sums every path forms, ordered_sum256.)
+constexpr int kWideThreads = 4 * kThreads;
+
+__global__ void __launch_bounds__(kWideThreads)
     bs_alpha(const SysRef* list, const int32_t* count, SysState* sys, const double* part_blk,
              int par) {
     __shared__ double2 red[kWarps + 1];
+    __shared__ double2 acc[8][kThreads];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const SysRef ref = list[i];
         SysState& S = sys[ref.slot];
         if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
-        const double pAp = ordered_sum256<false>(part_blk, ref.blk0, ref.blk1, red).x;
+        const double pAp = ordered_sum256_wide<false>(part_blk, ref.blk0, ref.blk1, acc, red).x;
         if (threadIdx.x == 0) S.alpha = pAp != 0.0 ? __ldcg(&S.rzp[par]) / pAp : 0.0;
     }
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kWideThreads)
     bs_beta(const SysRef* list, const int32_t* count, SysState* sys, const double* part_tile,
             int par, StepCtl* ctl) {
     __shared__ double2 red[kWarps + 1];
+    __shared__ double2 acc[8][kThreads];
     const int32_t n = __ldcg(count);
     for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const SysRef ref = list[i];
         SysState& S = sys[ref.slot];
         if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
-        const double2 t = ordered_sum256<true>(part_tile, ref.tile0, ref.tile1, red);
+        const double2 t = ordered_sum256_wide<true>(part_tile, ref.tile0, ref.tile1, acc, red);
         if (threadIdx.x == 0) {
             const double inner_rel = sqrt(t.y / S.rr0);
             const double est = S.rnorm * sqrt(t.y) / S.bnorm;
@@ -1196,13 +1269,13 @@ int launch_inner_body(nm_solver* S, cudaGraphConditionalHandle loop) {
         StepCtl* ctl = it == kLoopUnroll - 1 ? S->ctl : nullptr;
         bs_spmv_inner<V, T><<<g_spmv, kCtaThreads, smem, s>>>(M, p, Ap, S->st, S->part_blk,
                                                               S->err);
-        if (g_big) bs_alpha<<<g_big, kThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                       S->part_blk, par);
+        if (g_big) bs_alpha<<<g_big, kWideThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                           S->part_blk, par);
         bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->sblk, S->stile,
                                                 S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
                                                 par);
-        if (g_big) bs_beta<<<g_big, kThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                      S->part_tile, par, ctl);
+        if (g_big) bs_beta<<<g_big, kWideThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
+                                                          S->part_tile, par, ctl);
         bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
                                                  S->part_tile, z, p, par, ctl);
     }
