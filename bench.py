@@ -895,8 +895,13 @@ def run_engine(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         # the CPU solves in FP64: scale to the FP64 Jacobi-PCG iteration count
         # of this system (692, equal to the FP64 engine's)
+        got = {}
         line["cpu_baseline"] = cpu_baseline_cg(A, b, 1e-10, budget_s=args.cpu_seconds,
-                                               precond=True, full_iters=692)
+                                               precond=True, full_iters=692, out=got)
+        if "x" in got:  # the engine's solution against the oracle's FP64 Jacobi-PCG one
+            xo = got["x"]
+            line["config"]["rel_error_vs_oracle_solution"] = float(
+                np.linalg.norm(x - xo) / np.linalg.norm(xo))
     return line
 
 
@@ -1180,10 +1185,11 @@ def cpu_baseline_spmv(A, x, precision, budget_s=10.0):
                       f"{med * 1e3:.2f} ms; oracle/oracle.c or_spmv_*_omp (OpenMP static rows)"}
 
 
-def cpu_baseline_cg(A, b, tol, budget_s=10.0, precond=False, full_iters=None):
+def cpu_baseline_cg(A, b, tol, budget_s=10.0, precond=False, full_iters=None, out=None):
     """Threaded CPU CG (oracle/oracle.c or_cg_omp).  When one solve would take
     longer than the budget, a capped number of iterations is timed and the
-    solve time scaled to the full iteration count."""
+    solve time scaled to the full iteration count.  out (a dict): receives
+    the last full solve's x under "x" when full solves were timed."""
     from oracle import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
@@ -1197,10 +1203,12 @@ def cpu_baseline_cg(A, b, tol, budget_s=10.0, precond=False, full_iters=None):
         t_end = time.perf_counter() + budget_s
         while time.perf_counter() < t_end and len(times) < 200:
             t = time.perf_counter()
-            info, _ = oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=tol, max_iter=20000,
-                                    precond=precond)
+            info, xo = oracle.cg_omp(A.row_ptr, A.col_idx, A.values, b, tol=tol,
+                                     max_iter=20000, precond=precond)
             times.append(time.perf_counter() - t)
             iters = info["iters"]
+            if out is not None:
+                out["x"] = xo
         med = statistics.median(times)
         sample = (f"{len(times)} full solves ({iters} iterations each) in ~{budget_s:.0f} s, "
                   f"median {med * 1e3:.2f} ms")
