@@ -737,7 +737,8 @@ def cg_c1_measure(dev, steps, warmup, with_clock=True, local_rank=0, name="cg_c1
     _lib.load().nm_cg_last_path(M._h, C.byref(path))
     return {"A": A, "ms": ms, "iters": iters, "info": info, "max_err_vs_ones": err,
             "e2e_ms": e_ms, "h2d": bp.numel() * 8, "d2h": xp.numel() * 8,
-            "clocks": clk.summary() if clk else None, "path": CG_PATHS.get(path.value)}
+            "clocks": clk.summary() if clk else None, "path": CG_PATHS.get(path.value),
+            "path_id": path.value}
 
 
 CG_PATHS = {0: "CUDA-graph chunks of 3 kernels per iteration",
@@ -786,7 +787,10 @@ def run_cg(args, rank, world, local_rank):
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "ms_per_step": round(e2e_ms, 4),
                 "api": "kokkos_spmv.cg_solve_local with pinned b copied in and x copied out"},
-        "gpu_launches": int(r["iters"] * 3 + 2 * args.steps),
+        # per solve: A x0, the initial kernel, then one persistent launch, or
+        # three kernels per iteration on the CUDA-graph path
+        "gpu_launches": int(3 * args.steps if r["path_id"] in (1, 2, 3, 4)
+                            else r["iters"] * 3 + 2 * args.steps),
         "clocks": r["clocks"],
     })
     if world == 1 and not args.no_cpu_baseline:
