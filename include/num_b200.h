@@ -234,8 +234,9 @@ int nm_scale(int64_t n, double alpha, double* x, void* stream);
  * co-resident, else the resident solve (matrix rows and vectors kept on
  * chip, two grid-wide sums per iteration; rows of at most 8 nonzeros);
  * 2 the TMA-pipelined persistent solve only; 3 the resident solve only;
- * 4 the cluster solve only; 0 CUDA-graph chunks of three kernels per
- * iteration (also what 2 to 4 run where their path does not apply).  All
+ * 4 the cluster solve only; 0 CUDA-graph chunks of two kernels per
+ * iteration, the SpMV forming p = r + beta p as it reads it (also what 2 to 4
+ * run where their path does not apply).  All
  * give the same iterates, bit for bit (every dot product is summed in one
  * fixed order: per row block or 256-row tile, then over the blocks).  Other
  * values: NM_ERR_INVALID.  No reference counterpart (an implementation

@@ -244,6 +244,59 @@ struct CoopFormPApEpi {
     }
 };
 
+// Step 1 of the CUDA-graph path in its formed version (where the two sets of
+// staged windows fit the SM): the SpMV multiplies by p' = fma(beta, p_in, r)
+// formed from staged windows of both -- the operation the p update kernel
+// performs, on the same operands, in every CTA that reads a column -- each
+// row's owner writes p'[row] to p_out, and step 2 updates x with p_out; the
+// p update kernel goes.  The buffers alternate by iteration; the first
+// iteration of a solve forms fma(0, p0, r0) = r0 = p0 (beta is 0 in the
+// initial state), so the iterates are those of the three-kernel form.
+template <int TILE, int STAGES>
+__global__ void __launch_bounds__(kCtaThreads)
+    cg_spmv_pap_formed_kernel(const CsrView<double> M, CgState* st,
+                              const double* __restrict__ p_in, double* __restrict__ p_out,
+                              const double* __restrict__ r, double* __restrict__ Ap,
+                              double* partials, unsigned int* err) {
+    if (__ldcg(&st->done)) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& sm = *reinterpret_cast<SpmvSmem<double, double, double, TILE, STAGES, true>*>(smem_raw);
+    __shared__ bool am_last;
+    const double beta = __ldcg(&st->beta);
+    CoopFormPApEpi epi{Ap, p_in, r, p_out, partials, beta, 0.0};
+    const bool ok = spmv_pipeline<double, double, double, TILE, STAGES, true>(
+        M, p_in, sm, epi, err, AllBlocks(), r, beta);
+    if (!ok && threadIdx.x == 0) {
+        // A bounded wait gave up: end the solve; every CTA still arrives below
+        // so the arrival counter stays consistent.
+        atomicExch(&st->status, kCgDeviceError);
+        atomicExch(&st->done, 1);
+    }
+    // the last CTA to arrive adds the per-block sums in the fixed order
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        am_last = atomicAdd(&st->counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    const double pAp = reduce256(partials, M.nblk, sm.red);
+    if (threadIdx.x == 0) {
+        st->counter = 0u;
+        st->pAp = pAp;
+        if (st->guard && fabs(pAp) < 1e-300) {
+            st->status = kCgBreakdown;
+            st->done = 1;
+            st->converged = 0;
+            st->iters = st->iter;
+            st->final_res = sqrt(st->rr) / st->bnorm;
+        } else {
+            st->alpha = st->rr / pAp;
+        }
+    }
+}
+
 // FORMED: the two-barrier form.  Phase C disappears: the next iteration's
 // SpMV multiplies by p' = fma(beta, p, r) formed from staged windows of p and
 // r (the same operation on the same operands in every CTA that reads a
@@ -436,6 +489,19 @@ int prepare_cg_spmv(int* occ) {
                           occ);
 }
 
+template <int TILE, int STAGES>
+int prepare_cg_spmv_formed(int* occ) {
+    return prepare_kernel(
+        reinterpret_cast<const void*>(cg_spmv_pap_formed_kernel<TILE, STAGES>), kCtaThreads,
+        spmv_smem_bytes<double, double, double, TILE, STAGES, true>(), occ);
+}
+
+template <int TILE>
+int prepare_cg_spmv_formed_s(int stages, int* occ) {
+    if (stages == 4) return prepare_cg_spmv_formed<TILE, 4>(occ);
+    return stages == 3 ? prepare_cg_spmv_formed<TILE, 3>(occ) : prepare_cg_spmv_formed<TILE, 2>(occ);
+}
+
 template <int TILE, int STAGES, bool FORMED>
 int prepare_coop(int* occ) {
     return prepare_kernel(reinterpret_cast<const void*>(cg_coop_kernel<TILE, STAGES, FORMED>),
@@ -489,6 +555,17 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     }
     if (st != NM_OK) return st;
     ws->grid_spmv = spmv_grid(A, occ);
+    {
+        int occ_g = 0;
+        switch (A->tune.tile) {
+            case 1024: st = prepare_cg_spmv_formed_s<1024>(A->tune.stages, &occ_g); break;
+            case 4096: st = prepare_cg_spmv_formed_s<4096>(A->tune.stages, &occ_g); break;
+            default: st = prepare_cg_spmv_formed_s<2048>(A->tune.stages, &occ_g); break;
+        }
+        if (st != NM_OK) return st;
+        ws->graph_formed = occ_g > 0;
+        if (ws->graph_formed) ws->grid_spmv_f = spmv_grid(A, occ_g);
+    }
     // K1 leaves one sum per row block, K2 one per vector CTA, the initial
     // kernel two per vector CTA; the persistent solve keeps the block sums and
     // the vector sums side by side
@@ -538,10 +615,24 @@ int ensure_workspace(nm_csr* A, CgWorkspace** out) {
     return NM_OK;
 }
 
+// One iteration of the CUDA-graph path: three kernels, or (graph_formed) two,
+// the direction read from p (parity 0) or p2 (parity 1) and formed into the
+// other buffer.
 template <int TILE, int STAGES>
-void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s, int parity) {
     CsrView<double> M = A->view<double>();
-    M.stage_x = 1;  // p is a workspace vector (256-byte aligned)
+    M.stage_x = 1;  // p, p2 and r are workspace vectors (256-byte aligned)
+    if (ws->graph_formed) {
+        double* p_in = parity ? ws->p2 : ws->p;
+        double* p_out = parity ? ws->p : ws->p2;
+        cg_spmv_pap_formed_kernel<TILE, STAGES>
+            <<<ws->grid_spmv_f, kCtaThreads,
+               spmv_smem_bytes<double, double, double, TILE, STAGES, true>(), s>>>(
+                M, ws->st, p_in, p_out, ws->r, ws->Ap, ws->partials, ws->err);
+        cg_update_xr_kernel<<<ws->grid_vec, kThreads, 0, s>>>(ws->n, ws->st, p_out, ws->Ap,
+                                                              ws->r, ws->partials);
+        return;
+    }
     cg_spmv_pap_kernel<TILE, STAGES>
         <<<ws->grid_spmv, kCtaThreads, spmv_smem_bytes<double, double, double, TILE, STAGES>(), s>>>(
             M, ws->st, ws->p, ws->Ap, ws->partials, ws->err);
@@ -551,22 +642,22 @@ void launch_iteration_t(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
 }
 
 template <int TILE>
-void launch_iteration_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
-    if (A->tune.stages == 4) launch_iteration_t<TILE, 4>(A, ws, s);
-    else if (A->tune.stages == 3) launch_iteration_t<TILE, 3>(A, ws, s);
-    else launch_iteration_t<TILE, 2>(A, ws, s);
+void launch_iteration_s(const nm_csr* A, CgWorkspace* ws, cudaStream_t s, int parity) {
+    if (A->tune.stages == 4) launch_iteration_t<TILE, 4>(A, ws, s, parity);
+    else if (A->tune.stages == 3) launch_iteration_t<TILE, 3>(A, ws, s, parity);
+    else launch_iteration_t<TILE, 2>(A, ws, s, parity);
 }
 
-void launch_iteration(const nm_csr* A, CgWorkspace* ws, cudaStream_t s) {
+void launch_iteration(const nm_csr* A, CgWorkspace* ws, cudaStream_t s, int parity) {
     switch (A->tune.tile) {
-        case 1024: launch_iteration_s<1024>(A, ws, s); break;
-        case 4096: launch_iteration_s<4096>(A, ws, s); break;
-        default: launch_iteration_s<2048>(A, ws, s); break;
+        case 1024: launch_iteration_s<1024>(A, ws, s, parity); break;
+        case 4096: launch_iteration_s<4096>(A, ws, s, parity); break;
+        default: launch_iteration_s<2048>(A, ws, s, parity); break;
     }
 }
 
-// A CUDA graph of `iters` CG iterations (3 kernels each), captured once per
-// workspace and chunk length, replayed on the caller's stream.
+// A CUDA graph of `iters` CG iterations (2 or 3 kernels each), captured once
+// per workspace and chunk length, replayed on the caller's stream.
 int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* out) {
     auto it = ws->graphs.find(iters);
     if (it != ws->graphs.end()) {
@@ -577,7 +668,8 @@ int chunk_graph(const nm_csr* A, CgWorkspace* ws, int iters, cudaGraphExec_t* ou
     if (!ws->cap_stream)
         NM_CUDA_TRY(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
     NM_CUDA_TRY(cudaStreamBeginCapture(ws->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < iters; ++i) launch_iteration(A, ws, ws->cap_stream);
+    // chunks are of even length, so every chunk starts with the direction in p
+    for (int i = 0; i < iters; ++i) launch_iteration(A, ws, ws->cap_stream, i & 1);
     cudaError_t e = cudaStreamEndCapture(ws->cap_stream, &g);
     if (e != cudaSuccess) return fail(NM_ERR_CUDA, "CG graph capture failed: %s", cudaGetErrorString(e));
     cudaGraphExec_t ex = nullptr;

@@ -45,6 +45,8 @@ struct CgWorkspace {
     CgState* h_in = nullptr;    // pinned staging of the inputs (a slot of a shared slab)
     CgState* h_out = nullptr;   // pinned landing of the outputs (idem)
     int grid_spmv = 0, grid_vec = 0;
+    bool graph_formed = false;  // the graph path's SpMV forms p (two kernels per iteration)
+    int grid_spmv_f = 0;        // ... on this grid
     unsigned int* err = nullptr;  // device error word (not owned)
     cudaStream_t cap_stream = nullptr;
     std::map<int, cudaGraphExec_t> graphs;  // iterations per graph -> exec
