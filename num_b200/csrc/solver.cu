@@ -65,6 +65,8 @@ struct SysState {
     double rnorm_prev;  // scale of the previous inner solve
     double rz_keep;     // r.z of the last completed iteration of the previous inner solve
     double gamma;       // p = z + gamma p at an inner start (0: fresh start)
+    unsigned int tile_arrivals;  // large systems: tile CTAs of bs_update done this iteration
+    unsigned int pad2_;
 };
 
 struct SysRef {
@@ -95,8 +97,8 @@ constexpr int kTileRows = 4096;  // rows per vector-kernel tile (within one syst
 
 // A system is "large" when re-reducing its block sums in every tile CTA would
 // cost more than a couple of loads per thread: its alpha and beta are then
-// reduced once, by one CTA (bs_alpha / bs_beta), and the tile kernels read
-// them.  Tiles of a large system carry w = 1.  The choice depends only on the
+// reduced once -- alpha by one CTA (bs_alpha), beta by the last of its tile
+// CTAs in bs_update -- and the tile kernels read them.  Tiles of a large system carry w = 1.  The choice depends only on the
 // system's own size, so a system takes the same path alone and in any mix.
 constexpr int kLargeBlocks = 512;
 constexpr int kLargeTiles = 256;
@@ -463,37 +465,6 @@ __global__ void __launch_bounds__(kWideThreads)
     }
 }
 
-__global__ void __launch_bounds__(kWideThreads)
-    bs_beta(const SysRef* list, const int32_t* count, SysState* sys, const double* part_tile,
-            int par, StepCtl* ctl) {
-    __shared__ double2 red[kWarps + 1];
-    __shared__ double2 acc[8][kThreads];
-    const int32_t n = __ldcg(count);
-    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
-        const SysRef ref = list[i];
-        SysState& S = sys[ref.slot];
-        if (__ldcg(&S.phase) != kSysInner) continue;  // uniform over the CTA
-        const double2 t = ordered_sum256_wide<true>(part_tile, ref.tile0, ref.tile1, acc, red);
-        if (threadIdx.x == 0) {
-            const double inner_rel = sqrt(t.y / S.rr0);
-            const double est = S.rnorm * sqrt(t.y) / S.bnorm;
-            const bool stop = !(inner_rel > S.inner_rtol) || !(est >= S.stop_frac * S.tol) ||
-                              S.it_total >= S.max_iter;
-            const double rz_old = S.rzp[par];
-            S.rr = t.y;
-            if (stop) {
-                S.rz_keep = rz_old;
-                S.phase = kSysOuter;
-            } else {
-                S.beta = t.x / rz_old;
-                S.rzp[par ^ 1] = t.x;
-                if (ctl) atomicAdd(&ctl->live, 1u);
-            }
-        }
-        __syncthreads();
-    }
-}
-
 // ---- per-row vector steps over tiles {row0, row1, slot} ----------------------------
 //
 // A tile is up to kTileRows consecutive rows of one system; tiles start on
@@ -729,12 +700,47 @@ __global__ void __launch_bounds__(kThreads, 4)
     bs_update(const int4* tiles, const int32_t* count, SysState* sys, const int2* sblk,
               const int2* stile, const double* part_blk, const T* __restrict__ p,
               const T* __restrict__ Ap, const T* __restrict__ dinv, T* __restrict__ r,
-              T* __restrict__ z, T* __restrict__ d, double* part_tile, int par) {
+              T* __restrict__ z, T* __restrict__ d, double* part_tile, int par, StepCtl* ctl) {
     __shared__ double2 red[kWarps + 1];
+    __shared__ bool last;
     const int32_t i = blockIdx.x;
     if (i >= __ldcg(count)) return;
-    update_tile<T, false, false>(i, tiles[i], sys, sblk, stile, part_blk, p, Ap, dinv, r, z, d,
+    const int4 tl = tiles[i];
+    update_tile<T, false, false>(i, tl, sys, sblk, stile, part_blk, p, Ap, dinv, r, z, d,
                                  part_tile, par, red);
+    if (!tl.w) return;  // a small system: its tile CTAs decide in step 3
+    // A large system's stopping test and beta, by the last of its tile CTAs
+    // to finish (its tile sums in ordered_sum256's order, as the persistent
+    // step forms them), so the iteration needs no kernel of its own for them.
+    SysState& S = sys[tl.z];
+    const int2 tr = __ldg(stile + tl.z);
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's tile sum (and iteration count) before its arrival
+        last = atomicAdd(&S.tile_arrivals, 1u) == unsigned(tr.y - tr.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) S.tile_arrivals = 0u;
+    if (__ldcg(&S.phase) != kSysInner) return;  // uniform over the CTA
+    const double2 t = ordered_sum256<true>(part_tile, tr.x, tr.y, red);
+    if (threadIdx.x == 0) {
+        const double inner_rel = sqrt(t.y / __ldcg(&S.rr0));
+        const double est = __ldcg(&S.rnorm) * sqrt(t.y) / __ldcg(&S.bnorm);
+        const bool stop = !(inner_rel > __ldcg(&S.inner_rtol)) ||
+                          !(est >= __ldcg(&S.stop_frac) * __ldcg(&S.tol)) ||
+                          __ldcg(&S.it_total) >= __ldcg(&S.max_iter);
+        const double rz_old = __ldcg(&S.rzp[par]);
+        S.rr = t.y;
+        if (stop) {
+            S.rz_keep = rz_old;
+            S.phase = kSysOuter;
+        } else {
+            S.beta = t.x / rz_old;
+            S.rzp[par ^ 1] = t.x;
+            if (ctl) atomicAdd(&ctl->live, 1u);
+        }
+    }
 }
 
 // Inner iteration, step 3, for tile i: (r.z, r.r) of the system from its tile
@@ -744,7 +750,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 // another CTA of this step writes; the phase change of a stopping system is
 // the one write others may see early, and they then skip exactly as the test
 // would make them.  A continuing system's first tile counts it in *live.
-// SELF: a large system is decided here too, in bs_beta's order.
+// SELF: a large system is decided here too, in bs_update's order.
 template <typename T, bool COH, bool SELF>
 __device__ __forceinline__ void pupdate_tile(int32_t i, const int4 tl, SysState* sys,
                                              const int2* stile, const double* part_tile,
@@ -759,7 +765,7 @@ __device__ __forceinline__ void pupdate_tile(int32_t i, const int4 tl, SysState*
     __syncthreads();  // *sh is free for the next tile
     if (phase != kSysInner) return;  // uniform over the CTA
     double beta_d;
-    if (tl.w && !SELF) {  // large system: bs_beta ran the test and set beta (phase above)
+    if (tl.w && !SELF) {  // large system: bs_update ran the test and set beta (phase above)
         beta_d = __ldcg(&sys[slot].beta);
     } else {  // reduce the tile sums and decide, as every CTA of the system does
         const int2 tr = __ldg(stile + slot);
@@ -839,7 +845,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 // grid barrier after each phase -- the three phases the graph path launches as
 // kernels, with the same per-block / per-tile sums and the same per-system
 // reductions (ordered_sum256, also for large systems, whose alpha / beta the
-// graph path reduces in bs_alpha / bs_beta in the same order), so the two
+// graph path reduces in bs_alpha / bs_update in the same order), so the two
 // paths give the same bits.  Data written inside the launch is read through
 // L2.  After the third barrier every CTA reads how many systems go on (counted
 // by their first tiles into live2[parity]); the loop ends when none does or at
@@ -1054,7 +1060,7 @@ struct nm_solver {
     int64_t lists_gen = 0;   // bumped when the work-list arrays are reallocated
     int64_t graph_gen = -1;  // lists_gen the step graph was built against
     int graph_tiles = 0;     // tile grid of the step graph
-    bool graph_big = false;  // the step graph includes bs_alpha / bs_beta
+    bool graph_big = false;  // the step graph includes bs_alpha
     // pinned staging of admission uploads: a bump allocator, reset once the
     // stream has caught up (after each step's synchronisation)
     unsigned char* stage = nullptr;
@@ -1273,9 +1279,7 @@ int launch_inner_body(nm_solver* S, cudaGraphConditionalHandle loop) {
                                                            S->part_blk, par);
         bs_update<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->sblk, S->stile,
                                                 S->part_blk, p, Ap, dinv, r, z, d, S->part_tile,
-                                                par);
-        if (g_big) bs_beta<<<g_big, kWideThreads, 0, s>>>(S->bsys, &H->bsys, S->st,
-                                                          S->part_tile, par, ctl);
+                                                par, ctl);
         bs_pupdate<T><<<g_vec, kThreads, 0, s>>>(S->itile, &H->itile, S->st, S->stile,
                                                  S->part_tile, z, p, par, ctl);
     }
@@ -1320,7 +1324,6 @@ int prepare_solver_kernels(nm_solver* S) {
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pupdate<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_pstart<T>));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_alpha));
-    NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_beta));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_control));
     NM_CUDA_TRY(cudaFuncGetAttributes(&fa, bs_free_slots));
     int st = prepare_kernel(reinterpret_cast<const void*>(bs_spmv_inner<V, T>), kCtaThreads,
