@@ -70,10 +70,11 @@ struct CgWorkspace {
     ~CgWorkspace();
 };
 
-// The cluster solve: systems whose row blocks are whole 256-row tiles, of at
-// most 65,536 rows of at most 5 nonzeros (49,152 of 7 or 8 when every value
-// is a float exactly, 40,960 otherwise), on one cluster of 16 CTAs when the
-// device can schedule it and the rows fit its shared memory.  NM_OK with
+// The cluster solve: systems whose row blocks are whole 256-row tiles and
+// whose rows fit the cluster's shared memory -- when every value is a float
+// exactly, at most 65,536 rows of at most 5 nonzeros or 49,152 of 7 or 8;
+// otherwise about 57,000 rows of at most 5 or 40,960 of 7 or 8 -- on one
+// cluster of 16 CTAs when the device can schedule it.  NM_OK with
 // ws->cluster false when it cannot.
 int plan_cluster(const nm_csr* A, CgWorkspace* ws);
 // One cluster solve on `s` after cg_init_kernel (ws->r, ws->p hold r0 = p0).
