@@ -1318,7 +1318,8 @@ def run_reference(args, rank, world):
         cb = cpu_baseline_cg(A, b, tol, budget_s=per_step_budget * args.steps, precond=pre,
                              full_iters=iters)
         val, unit, sample = cb["value"], "solves/s", cb["sample"] + f" ({note})"
-        cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz}
+        cfg = {"workload": desc, "name": args.workload, "nrows": A.nrows, "nnz": A.nnz,
+               "tol": tol}
         ms_step = 1e3 / val
     elif kind == "vec":
         from oracle import oracle
