@@ -899,7 +899,10 @@ def run_engine(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(A.nnz * (12 + vb) + A.nrows * 16),
                 "d2h_bytes_per_step": int(A.nrows * 8), "ms_per_step": round(e_ms, 3),
                 "api": "BatchSolver.solve: admission from host arrays, steps, take"},
-        "gpu_launches": int((c1["inner_iterations"] - c0["inner_iterations"]) * 3 +
+        # per inner iteration of the one large system: SpMV, alpha, update, p
+        # update; one control kernel per 8-iteration body; the refinement steps
+        "gpu_launches": int((c1["inner_iterations"] - c0["inner_iterations"]) * 4 +
+                            (c1["inner_iterations"] - c0["inner_iterations"]) // 8 +
                             (c1["outer_launches"] - c0["outer_launches"]) * 6),
         "clocks": clk.summary(),
     })
@@ -1068,7 +1071,11 @@ def run_serve(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(tot_rows * 8),
                 "note": "the served loop is end to end by construction: every request's "
                         "matrix and b come from host memory and x goes back"},
+        # at least SpMV, update, p update per inner iteration (alpha too while
+        # a large system is live), one control kernel per 8-iteration body,
+        # the refinement steps
         "gpu_launches": int((c1["inner_iterations"] - c0["inner_iterations"]) * 3 +
+                            (c1["inner_iterations"] - c0["inner_iterations"]) // 8 +
                             (c1["outer_launches"] - c0["outer_launches"]) * 6),
         "clocks": r["clocks"],
     })
