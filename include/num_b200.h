@@ -200,6 +200,21 @@ int nm_row_blocks_host(const int32_t* row_ptr, int32_t nrows, const nm_tuning* t
  * accumulate in FP32. */
 int nm_spmv(const nm_csr* A, const void* x, void* y, void* stream);
 
+/* y = A*x for x[ncols] and y[nrows] in HOST memory (element types as for
+ * nm_spmv): copies x in, multiplies, copies y out and returns when y is
+ * written -- the work is ordered after what is already queued on `stream`,
+ * and `stream` is synchronised before the call returns, also after an error.
+ * The row blocks run in chunks, each as soon as the part of x its nonzeros
+ * read has arrived, and each chunk's rows of y are copied out while later
+ * chunks compute, so for banded matrices the two transfers overlap
+ * (page-locked x and y let the copies run at the full link rate).  The handle
+ * keeps device copies of x and y (allocated on the first call, freed with the
+ * handle); calls on one handle run one after the other.  Addition: the
+ * reference's spmv takes device arrays only (src/bindings.cpp:152-183); this
+ * is the call for a host-side caller, who would otherwise copy x in and y out
+ * around nm_spmv. */
+int nm_spmv_host(const nm_csr* A, const void* x, void* y, void* stream);
+
 /* batch_spmv(A, X, Y) (src/bindings.cpp:186-200; launch_batch_spmv,
  * src/batch_spmv_kernel.hpp:120-174): Y(nrows,k) = A * X(ncols,k), both
  * row-major.  F64 matrices only (as in the reference). */

@@ -73,6 +73,7 @@ _SIGNATURES = {
     "nm_csr_row_blocks": ([vp, vp, i32, vp], C.c_int),
     "nm_row_blocks_host": ([vp, i32, C.POINTER(Tuning), vp, i32, vp, P_i32], C.c_int),
     "nm_spmv": ([vp, vp, vp, vp], C.c_int),
+    "nm_spmv_host": ([vp, vp, vp, vp], C.c_int),
     "nm_batch_spmv": ([vp, vp, vp, i32, vp], C.c_int),
     "nm_axpy": ([i64, dbl, vp, vp, vp, vp], C.c_int),
     "nm_axpy2": ([i64, dbl, vp, dbl, vp, vp, vp], C.c_int),

@@ -173,6 +173,7 @@ int upload(nm_csr* A, const int32_t* rp, const int32_t* ci, const void* vals) {
 }  // namespace
 
 int rebuild_blocks(nm_csr* A) {
+    ++A->layout_gen;
     std::vector<int32_t> blk;
     A->nblk = build_row_blocks(A->h_row_ptr.data(), A->nrows, A->tune.tile, A->tune.max_rows,
                                A->tune.short_max, blk, nullptr);
@@ -280,6 +281,7 @@ int spmv_grid(const nm_csr* A, int ctas_per_sm) {
 
 nm_csr::~nm_csr() {
     cg.reset();
+    host_spmv.reset();
     if (d_row_ptr) cudaFree(d_row_ptr);
     if (d_col_idx) cudaFree(d_col_idx);
     if (d_values) cudaFree(d_values);

@@ -77,6 +77,26 @@ void block_xwindows(const int32_t* col_idx, int32_t z0, int32_t z1, int32_t ncol
 int build_row_blocks(const int32_t* row_ptr, int32_t nrows, int tile, int max_rows,
                      int short_max, std::vector<int32_t>& blk, std::vector<int8_t>* bins);
 
+// State of nm_spmv_host (spmv.cu) on one handle, made on its first call: the
+// device copies of x and y, a copy-in and a copy-out stream, and the split of
+// x into pieces and of the row blocks into chunks, each chunk with the last x
+// piece its nonzeros read.
+struct HostSpmv {
+    std::mutex mu;  // one call at a time on the handle
+    void* dx = nullptr;
+    void* dy = nullptr;
+    cudaStream_t in = nullptr, out = nullptr;
+    cudaEvent_t begin = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> x_ready;  // per x piece
+    std::vector<cudaEvent_t> y_ready;  // per row chunk
+    uint32_t gen = ~0u;                // nm_csr::layout_gen the split was made for
+    std::vector<int64_t> xcut;         // x piece p: elements [xcut[p], xcut[p+1])
+    std::vector<int32_t> blk;          // row chunk c: blocks [blk[c], blk[c+1])
+    std::vector<int32_t> row;          // row chunk c: rows [row[c], row[c+1])
+    std::vector<int32_t> need;         // row chunk c reads x pieces 0..need[c] (-1: none)
+    ~HostSpmv();
+};
+
 }  // namespace nm
 
 struct nm_csr {
@@ -113,8 +133,12 @@ struct nm_csr {
     std::vector<int32_t> h_col_idx;  // kept to rebuild the x windows on retuning
     // Many-matrix handles: per-matrix row / column offsets (count + 1 each).
     std::vector<int32_t> batch_row_off, batch_col_off;
+    // Incremented by every rebuild of the row-block partition.
+    uint32_t layout_gen = 0;
     std::mutex cg_mutex;
     std::unique_ptr<nm::CgWorkspace> cg;
+    mutable std::mutex host_mutex;  // guards host_spmv's creation
+    mutable std::unique_ptr<nm::HostSpmv> host_spmv;
     ~nm_csr();
 
     template <typename V>

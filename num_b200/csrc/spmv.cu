@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <new>
 #include <vector>
 
 namespace nm {
@@ -309,9 +310,16 @@ int build_sell(nm_csr* A) {
     return NM_OK;
 }
 
+// nb >= 0: only the row blocks [b0, b0 + nb) (their rows of y are written,
+// no others).
 template <typename V, typename X, typename A, int TILE, int STAGES>
-static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
+static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s, int32_t b0,
+                       int32_t nb) {
     CsrView<V> M = Am->view<V>();
+    if (nb >= 0) {
+        M.desc += b0;
+        M.nblk = nb;
+    }
     M.stage_x = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
     constexpr size_t smem = spmv_smem_bytes<V, X, A, TILE, STAGES>();
     auto* fn = spmv_kernel<V, X, A, TILE, STAGES>;
@@ -320,7 +328,7 @@ static int launch_tile(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
     if (st != NM_OK) return st;
     unsigned int* err = device_error_word();
     if (!err) return fail(NM_ERR_CUDA, "spmv: cannot map the device error word");
-    const int grid = spmv_grid(Am, occ);
+    const int grid = std::max(1, std::min(spmv_grid(Am, occ), M.nblk));
     fn<<<grid, kCtaThreads, smem, s>>>(M, x, y, err);
     NM_CHECK_LAUNCH();
     return NM_OK;
@@ -384,22 +392,27 @@ int launch_spmv_rows(const nm_csr* A, const double* x, double* y, const int32_t*
 }
 
 template <typename V, typename X, typename A, int TILE>
-static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    if (Am->tune.stages == 4) return launch_tile<V, X, A, TILE, 4>(Am, x, y, s);
-    if (Am->tune.stages == 3) return launch_tile<V, X, A, TILE, 3>(Am, x, y, s);
-    return launch_tile<V, X, A, TILE, 2>(Am, x, y, s);
+static int launch_stages(const nm_csr* Am, const X* x, X* y, cudaStream_t s, int32_t b0,
+                         int32_t nb) {
+    if (Am->tune.stages == 4) return launch_tile<V, X, A, TILE, 4>(Am, x, y, s, b0, nb);
+    if (Am->tune.stages == 3) return launch_tile<V, X, A, TILE, 3>(Am, x, y, s, b0, nb);
+    return launch_tile<V, X, A, TILE, 2>(Am, x, y, s, b0, nb);
 }
 
+// nb >= 0: the row blocks [b0, b0 + nb) of the row-block kernel only.
 template <typename V, typename X, typename A>
-static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s) {
-    if (Am->warp_gather)
+static int launch_typed(const nm_csr* Am, const X* x, X* y, cudaStream_t s, int32_t b0 = 0,
+                        int32_t nb = -1) {
+    if (Am->warp_gather) {
+        if (nb >= 0) return fail(NM_ERR_RUNTIME, "spmv: block range on the gather kernel");
         return Am->tune.kernel == NM_KERNEL_SLICED && Am->sell_ready
                    ? launch_sell<V, X, A>(Am, x, y, s)
                    : launch_gather<V, X, A>(Am, x, y, s);
+    }
     switch (Am->tune.tile) {
-        case 1024: return launch_stages<V, X, A, 1024>(Am, x, y, s);
-        case 2048: return launch_stages<V, X, A, 2048>(Am, x, y, s);
-        case 4096: return launch_stages<V, X, A, 4096>(Am, x, y, s);
+        case 1024: return launch_stages<V, X, A, 1024>(Am, x, y, s, b0, nb);
+        case 2048: return launch_stages<V, X, A, 2048>(Am, x, y, s, b0, nb);
+        case 4096: return launch_stages<V, X, A, 4096>(Am, x, y, s, b0, nb);
         default: return fail(NM_ERR_INVALID, "spmv: unsupported tile %d", Am->tune.tile);
     }
 }
@@ -433,19 +446,25 @@ size_t spmv_smem_for(int dtype, int tile, int stages) {
     }
 }
 
-int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
+// nb >= 0: the row blocks [b0, b0 + nb) only (row-block kernel).
+static int launch_spmv_range(const nm_csr* A, const void* x, void* y, int32_t b0, int32_t nb,
+                             cudaStream_t s) {
     switch (A->dtype) {
         case NM_F64:
             return launch_typed<double, double, double>(A, static_cast<const double*>(x),
-                                                        static_cast<double*>(y), s);
+                                                        static_cast<double*>(y), s, b0, nb);
         case NM_F32:
             return launch_typed<float, float, float>(A, static_cast<const float*>(x),
-                                                     static_cast<float*>(y), s);
+                                                     static_cast<float*>(y), s, b0, nb);
         case NM_BF16:
             return launch_typed<__nv_bfloat16, float, float>(A, static_cast<const float*>(x),
-                                                             static_cast<float*>(y), s);
+                                                             static_cast<float*>(y), s, b0, nb);
         default: return fail(NM_ERR_TYPE, "spmv: unknown dtype %d", A->dtype);
     }
+}
+
+int launch_spmv(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
+    return launch_spmv_range(A, x, y, 0, -1, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -733,9 +752,205 @@ static int launch_batch(const nm_csr* A, const double* X, double* Y, int32_t k, 
     return NM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// y = A x with x and y in host memory (nm_spmv_host).
+//
+// x goes in as pieces on one stream and y comes out as chunks on another; the
+// row blocks run in chunks on the caller's stream, each after the x pieces up
+// to the last one its nonzeros read (found once per partition from the host
+// copy of the column indices), and each chunk's rows of y leave while the
+// next chunks compute.  A banded matrix's chunk waits for about one piece
+// beyond its own rows, so the copy-out runs beside the copy-in and the call
+// takes about one direction's transfer time instead of both.  The
+// warp-gather kernels (scattered columns: every chunk would wait for all of
+// x) and vectors of under two pieces run as one copy in, one SpMV, one copy
+// out.
+// ---------------------------------------------------------------------------
+
+HostSpmv::~HostSpmv() {
+    for (cudaEvent_t e : x_ready) cudaEventDestroy(e);
+    for (cudaEvent_t e : y_ready) cudaEventDestroy(e);
+    if (begin) cudaEventDestroy(begin);
+    if (done) cudaEventDestroy(done);
+    if (in) cudaStreamDestroy(in);
+    if (out) cudaStreamDestroy(out);
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+}
+
+namespace {
+
+constexpr int64_t kHostPieceBytes = int64_t(2) << 20;  // x piece / y chunk size aimed at
+constexpr int kHostMaxPieces = 16;
+// A chunk also waits for the x elements up to this far past its largest
+// column (the staged x windows end on multiples of 4 elements).
+constexpr int64_t kHostXMargin = 8;
+
+int host_vec_bytes(int dtype) { return dtype == NM_F64 ? 8 : 4; }
+
+int host_pieces(int64_t n, int esz) {
+    return int(std::max<int64_t>(1, std::min<int64_t>(kHostMaxPieces, n * esz / kHostPieceBytes)));
+}
+
+int grow_events(std::vector<cudaEvent_t>& ev, size_t n) {
+    while (ev.size() < n) {
+        cudaEvent_t e = nullptr;
+        NM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev.push_back(e);
+    }
+    return NM_OK;
+}
+
+// The split of x into pieces and of the row blocks into chunks (no chunks:
+// one copy in, one SpMV, one copy out).
+int plan_host_spmv(const nm_csr* A, HostSpmv* h) {
+    const int esz = host_vec_bytes(A->dtype);
+    h->xcut.clear();
+    h->blk.clear();
+    h->row.clear();
+    h->need.clear();
+    const int P = host_pieces(A->ncols, esz);
+    const int C = std::min(host_pieces(A->nrows, esz), std::max(1, A->nblk));
+    if (A->warp_gather || P < 2 || C < 2) return NM_OK;
+    if (A->h_row_ptr.size() != size_t(A->nrows) + 1 || A->h_col_idx.size() < size_t(A->nnz))
+        return NM_OK;  // no host copy of the pattern to find each chunk's columns
+    for (int p = 0; p < P; ++p) {
+        const int64_t c = (int64_t(A->ncols) * p / P) & ~int64_t(63);
+        if (h->xcut.empty() || c > h->xcut.back()) h->xcut.push_back(c);
+    }
+    h->xcut.push_back(A->ncols);
+    std::vector<int32_t> bh(size_t(A->nblk) + 1);
+    NM_CUDA_TRY(cudaMemcpy(bh.data(), A->d_blk, sizeof(int32_t) * bh.size(),
+                           cudaMemcpyDeviceToHost));
+    h->blk.push_back(0);
+    h->row.push_back(0);
+    for (int c = 1; c < C; ++c) {
+        const int64_t target = int64_t(A->nrows) * c / C;
+        const int32_t b = int32_t(std::lower_bound(bh.begin(), bh.end(), target) - bh.begin());
+        if (b <= h->blk.back() || b >= A->nblk) continue;
+        h->blk.push_back(b);
+        h->row.push_back(bh[b]);
+    }
+    h->blk.push_back(A->nblk);
+    h->row.push_back(A->nrows);
+    const int32_t* rp = A->h_row_ptr.data();
+    const int32_t* ci = A->h_col_idx.data();
+    for (size_t c = 0; c + 1 < h->blk.size(); ++c) {
+        int32_t mx = -1;
+        for (int32_t z = rp[h->row[c]]; z < rp[h->row[c + 1]]; ++z) mx = std::max(mx, ci[z]);
+        int32_t need = -1;
+        if (mx >= 0) {
+            const int64_t last = std::min<int64_t>(int64_t(mx) + kHostXMargin, A->ncols - 1);
+            need = int32_t(std::upper_bound(h->xcut.begin(), h->xcut.end(), last) -
+                           h->xcut.begin()) - 1;
+        }
+        h->need.push_back(need);
+    }
+    int st = grow_events(h->x_ready, h->xcut.size() - 1);
+    if (st == NM_OK) st = grow_events(h->y_ready, h->blk.size() - 1);
+    return st;
+}
+
+int spmv_host(const nm_csr* A, const void* x, void* y, cudaStream_t s) {
+    HostSpmv* h = nullptr;
+    {
+        std::lock_guard<std::mutex> g(A->host_mutex);
+        if (!A->host_spmv) A->host_spmv.reset(new (std::nothrow) HostSpmv());
+        h = A->host_spmv.get();
+    }
+    if (!h) return fail(NM_ERR_NOMEM, "spmv_host: out of host memory");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (A->nrows == 0) return NM_OK;
+    const int esz = host_vec_bytes(A->dtype);
+    const size_t xb = size_t(A->ncols) * esz, yb = size_t(A->nrows) * esz;
+    if (!h->dx && cudaMalloc(&h->dx, std::max<size_t>(xb, 16)) != cudaSuccess) {
+        cudaGetLastError();
+        h->dx = nullptr;
+        return fail(NM_ERR_NOMEM, "spmv_host: cannot allocate the device x (%zu bytes)", xb);
+    }
+    if (!h->dy && cudaMalloc(&h->dy, yb) != cudaSuccess) {
+        cudaGetLastError();
+        h->dy = nullptr;
+        return fail(NM_ERR_NOMEM, "spmv_host: cannot allocate the device y (%zu bytes)", yb);
+    }
+    if (!h->in) NM_CUDA_TRY(cudaStreamCreateWithFlags(&h->in, cudaStreamNonBlocking));
+    if (!h->out) NM_CUDA_TRY(cudaStreamCreateWithFlags(&h->out, cudaStreamNonBlocking));
+    if (!h->begin) NM_CUDA_TRY(cudaEventCreateWithFlags(&h->begin, cudaEventDisableTiming));
+    if (!h->done) NM_CUDA_TRY(cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming));
+    if (h->gen != A->layout_gen) {
+        const int st = plan_host_spmv(A, h);
+        if (st != NM_OK) return st;
+        h->gen = A->layout_gen;
+    }
+    int st = NM_OK;
+    auto cu = [&](cudaError_t e, const char* what) {
+        if (st == NM_OK && e != cudaSuccess)
+            st = fail(NM_ERR_CUDA, "spmv_host: %s failed: %s", what, cudaGetErrorString(e));
+    };
+    char* dx = static_cast<char*>(h->dx);
+    char* dy = static_cast<char*>(h->dy);
+    if (h->blk.empty()) {
+        if (xb) cu(cudaMemcpyAsync(dx, x, xb, cudaMemcpyHostToDevice, s), "copy of x");
+        if (st == NM_OK) st = launch_spmv(A, dx, dy, s);
+        if (st == NM_OK) cu(cudaMemcpyAsync(y, dy, yb, cudaMemcpyDeviceToHost, s), "copy of y");
+        const cudaError_t e = cudaStreamSynchronize(s);
+        cu(e, "stream synchronize");
+        return st;
+    }
+    // Both copy streams start after the work already queued on s.
+    cu(cudaEventRecord(h->begin, s), "event record");
+    cu(cudaStreamWaitEvent(h->in, h->begin, 0), "stream wait");
+    cu(cudaStreamWaitEvent(h->out, h->begin, 0), "stream wait");
+    const char* xh = static_cast<const char*>(x);
+    char* yh = static_cast<char*>(y);
+    for (size_t p = 0; st == NM_OK && p + 1 < h->xcut.size(); ++p) {
+        const int64_t a = h->xcut[p], b = h->xcut[p + 1];
+        cu(cudaMemcpyAsync(dx + a * esz, xh + a * esz, size_t(b - a) * esz,
+                           cudaMemcpyHostToDevice, h->in), "copy of x");
+        cu(cudaEventRecord(h->x_ready[p], h->in), "event record");
+    }
+    int32_t waited = -1;  // the x pieces 0..waited are known to be in for s
+    for (size_t c = 0; st == NM_OK && c + 1 < h->blk.size(); ++c) {
+        if (h->need[c] > waited) {
+            cu(cudaStreamWaitEvent(s, h->x_ready[h->need[c]], 0), "stream wait");
+            waited = h->need[c];
+        }
+        if (st != NM_OK) break;
+        st = launch_spmv_range(A, dx, dy, h->blk[c], h->blk[c + 1] - h->blk[c], s);
+        if (st != NM_OK) break;
+        cu(cudaEventRecord(h->y_ready[c], s), "event record");
+        cu(cudaStreamWaitEvent(h->out, h->y_ready[c], 0), "stream wait");
+        const int64_t r0 = h->row[c], r1 = h->row[c + 1];
+        if (r1 > r0)
+            cu(cudaMemcpyAsync(yh + r0 * esz, dy + r0 * esz, size_t(r1 - r0) * esz,
+                               cudaMemcpyDeviceToHost, h->out), "copy of y");
+    }
+    cu(cudaEventRecord(h->done, h->out), "event record");
+    cu(cudaStreamWaitEvent(s, h->done, 0), "stream wait");
+    // Everything this call queued has finished before it returns, also after
+    // a failure (the host buffers are the caller's again).
+    const cudaError_t e1 = cudaStreamSynchronize(h->in);
+    const cudaError_t e2 = cudaStreamSynchronize(h->out);
+    const cudaError_t e3 = cudaStreamSynchronize(s);
+    cu(e1, "stream synchronize");
+    cu(e2, "stream synchronize");
+    cu(e3, "stream synchronize");
+    return st;
+}
+
+}  // namespace
+
 }  // namespace nm
 
 using nm::fail;
+
+extern "C" int nm_spmv_host(const nm_csr* A, const void* x, void* y, void* stream) {
+    nm::clear_error();
+    if (!A) return fail(NM_ERR_INVALID, "nm_spmv_host: NULL matrix");
+    if ((!x && A->ncols > 0) || (!y && A->nrows > 0))
+        return fail(NM_ERR_INVALID, "nm_spmv_host: NULL argument");
+    return nm::spmv_host(A, x, y, static_cast<cudaStream_t>(stream));
+}
 
 extern "C" int nm_spmv(const nm_csr* A, const void* x, void* y, void* stream) {
     nm::clear_error();

@@ -34,9 +34,9 @@ except ImportError:  # pragma: no cover
 
 __all__ = [
     "init", "finalize", "rank", "size", "barrier", "CrsMatrix", "DistCrsMatrix", "upload_csr",
-    "upload_csr_batched", "distribute_csr", "spmv", "batch_spmv", "dist_spmv", "cg_solve",
-    "cg_solve_local", "tune", "tuning", "autotune", "row_blocks", "laplacian", "download_csr",
-    "spmv_kernel",
+    "upload_csr_batched", "distribute_csr", "spmv", "spmv_host", "batch_spmv", "dist_spmv",
+    "cg_solve", "cg_solve_local", "tune", "tuning", "autotune", "row_blocks", "laplacian",
+    "download_csr", "spmv_kernel",
 ]
 
 _PRECISIONS = {"fp64": _lib.NM_F64, "fp32": _lib.NM_F32, "bf16": _lib.NM_BF16}
@@ -331,6 +331,33 @@ def spmv(A: CrsMatrix, x, y, kokkoskernels: bool = True, *, async_: bool = False
     if not async_:
         torch.cuda.current_stream(yt.device).synchronize()
         _lib.check(lib.nm_check_device_errors(), "spmv")
+
+
+def spmv_host(A: CrsMatrix, x, y) -> None:
+    """y = A @ x with x and y in host memory (numpy arrays or CPU tensors;
+    float64 for fp64 matrices, float32 for fp32/bf16 ones), through the C
+    ABI's nm_spmv_host: x is copied in and y out around the SpMV, the row
+    blocks in chunks so that the two copies overlap, and the call returns when
+    y is written.  Page-locked arrays (torch `pin_memory()`) let the copies
+    run at the full link rate.  y must be contiguous and writable.  Addition:
+    the reference's spmv takes device arrays only."""
+    dt = _vec_dtype(A)
+    xa = host_array(x, dt, "x")
+    if isinstance(y, np.ndarray):
+        if not (y.flags.c_contiguous and y.flags.writeable):
+            raise ValueError("spmv_host: y must be a contiguous, writable array")
+    elif torch is not None and isinstance(y, torch.Tensor):
+        if y.device.type == "cpu" and not y.is_contiguous():
+            raise ValueError("spmv_host: y must be contiguous")
+    ya = host_array(y, dt, "y")
+    if xa.shape[0] != A.ncols:
+        raise ValueError("spmv_host: x length != A.ncols")
+    if ya.shape[0] != A.nrows:
+        raise ValueError("spmv_host: y length != A.nrows")
+    lib = _lib.load()
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.nm_spmv_host(A._h, xa.ctypes.data, ya.ctypes.data, s), "spmv_host")
+    _lib.check(lib.nm_check_device_errors(), "spmv_host")
 
 
 def batch_spmv(A: CrsMatrix, X, Y, *, async_: bool = False) -> None:
