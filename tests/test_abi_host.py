@@ -201,3 +201,11 @@ def test_tune_kernel_names_checked_on_host(nmlib):
     from num_b200 import _lib
     assert st == _lib.NM_ERR_INVALID
 
+
+
+def test_spmv_host_null_arguments_rejected_on_host(nmlib):
+    """nm_spmv_host checks its pointers before any device call."""
+    from num_b200 import _lib
+    y = np.empty(4)
+    assert nmlib.nm_spmv_host(None, y.ctypes.data, y.ctypes.data, None) == _lib.NM_ERR_INVALID
+    assert b"NULL" in nmlib.nm_last_error()
