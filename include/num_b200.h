@@ -209,7 +209,8 @@ int nm_spmv(const nm_csr* A, const void* x, void* y, void* stream);
  * chunks compute, so for banded matrices the two transfers overlap
  * (page-locked x and y let the copies run at the full link rate).  The handle
  * keeps device copies of x and y (allocated on the first call, freed with the
- * handle); calls on one handle run one after the other.  Addition: the
+ * handle); calls on one handle run one after the other.  Not callable on a
+ * stream that is being captured (it synchronises the stream).  Addition: the
  * reference's spmv takes device arrays only (src/bindings.cpp:152-183); this
  * is the call for a host-side caller, who would otherwise copy x in and y out
  * around nm_spmv. */
